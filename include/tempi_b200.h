@@ -1,0 +1,152 @@
+/* tempi_b200.h -- the drop-in boundary of libtempi_b200.so.
+
+   Two surfaces:
+
+   1. Interposed MPI entry points.  libtempi_b200.so exports these MPI-3.1
+      functions with their standard C signatures (declared by the MPI
+      library's own mpi.h, so they are listed here only as a comment).  An
+      application links libtempi_b200.so ahead of its MPI library, or
+      preloads it; each call reaches the real MPI through
+      dlsym(RTLD_NEXT, name) when TEMPI cannot or should not handle it.
+
+        MPI_Init          replaces reference src/init.cpp:22-67
+        MPI_Init_thread   replaces reference src/init_thread.cpp:22-65
+        MPI_Finalize      replaces reference src/finalize.cpp:20-46
+        MPI_Type_commit   replaces reference src/type_commit.cpp:16-114
+        MPI_Type_free     replaces reference src/type_free.cpp:14-26
+        MPI_Pack          replaces reference src/pack.cpp:28-68
+        MPI_Unpack        replaces reference src/unpack.cpp:20-60
+        MPI_Send          replaces reference src/send.cpp + src/internal/send.cpp:21-53
+        MPI_Recv          replaces reference src/recv.cpp:19-52
+        MPI_Isend         replaces reference src/isend.cpp + src/internal/isend.cpp:15-45
+        MPI_Irecv         replaces reference src/irecv.cpp + src/internal/irecv.cpp:15-44
+        MPI_Wait          replaces reference src/wait.cpp:11-16
+
+      Signatures are those of include/symbols.hpp in the reference
+      (PARAMS_MPI_* macros, lines 10-178).
+
+   2. The thin kernel ABI below: plain pointers and sizes, no MPI or torch
+      types, every function returning 0 (TEMPI_OK) or a TEMPI_ERR_* code.
+      The MPI layer is built on it; tests, benchmarks and non-MPI callers use
+      it directly.
+*/
+#ifndef TEMPI_B200_H
+#define TEMPI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TEMPI_OK 0
+#define TEMPI_ERR_ARG 1         /* bad argument or descriptor */
+#define TEMPI_ERR_CUDA 2        /* a CUDA call failed (message via tempi_last_error) */
+#define TEMPI_ERR_UNSUPPORTED 3 /* type cannot be described as a strided block */
+#define TEMPI_ERR_TIMEOUT 4     /* a bounded wait ran out */
+#define TEMPI_ERR_NO_MEM 5
+#define TEMPI_ERR_TRUNCATE 6    /* output buffer too small */
+#define TEMPI_ERR_NOT_BUILT 7   /* compiled without the kernel */
+
+#define TEMPI_MAX_DIMS 4
+
+/* A canonical strided block: the bytes of one object are
+     for i[nd-1] .. for i[0]: copy `block` bytes from
+       origin + start + sum_k i[k]*strides[k]
+   in that order (counts[0]/strides[0] vary fastest).  Object j of a
+   multi-object call starts at origin + j*extent.  `align` is the largest
+   power of two <= 16 dividing start, block, every stride and extent.  The
+   same information as the reference's StridedBlock
+   (include/strided_block.hpp:12-67), whose counts[0] is the block length. */
+typedef struct tempi_desc {
+  int64_t start;
+  int64_t extent;
+  int64_t block;
+  int64_t size; /* packed bytes of one object = block * prod(counts) */
+  int32_t ndims;
+  int32_t align;
+  int64_t counts[TEMPI_MAX_DIMS];
+  int64_t strides[TEMPI_MAX_DIMS];
+} tempi_desc;
+
+/* Kernel choice for one launch.  Zero fields mean "let the library pick".
+   kernel: 0 auto, 1 word kernel, 2 row kernel.  width: vector bytes
+   (1,2,4,8,16; never above what the alignment proof allows). */
+typedef struct tempi_config {
+  int32_t kernel;
+  int32_t width;
+  int32_t threads;
+  int32_t unroll;
+  int32_t blocks_per_sm;
+  int32_t reserved;
+} tempi_config;
+
+/* ---- strided pack / unpack (reference Packer::pack/unpack_async,
+        include/packer.hpp:14-49; kernels pack_kernels.cuh:64-120, 350-433) */
+
+/* Pack `incount` objects described by `d` from `origin` (device-accessible)
+   into `packed` (device-accessible, incount*d->size bytes).  Asynchronous
+   on `stream` (a cudaStream_t; 0 = legacy default stream). */
+int tempi_pack(const tempi_desc *d, const void *origin, int64_t incount,
+               void *packed, const tempi_config *cfg, void *stream);
+/* Inverse of tempi_pack; bytes of `origin` outside the description are
+   never written. */
+int tempi_unpack(const tempi_desc *d, const void *packed, int64_t incount,
+                 void *origin, const tempi_config *cfg, void *stream);
+
+/* Canonicalise a committed MPI datatype handle (MPI_Datatype passed as an
+   integer or pointer-sized value) the way MPI_Type_commit does.  Returns
+   TEMPI_ERR_UNSUPPORTED if the type is not a strided block. */
+int tempi_describe(int64_t datatype, tempi_desc *out);
+
+/* ---- batched pack: many (object, region) pairs in one launch -------------
+   A region is `incount` objects of a strided block whose typed buffer has
+   its origin at `origin`, packed to (or unpacked from) `packed`.  The table
+   lives in device memory, so a captured graph replays with new data and no
+   re-capture.  No counterpart in the reference, which packs one object per
+   launch (src/pack.cpp:56). */
+typedef struct tempi_region {
+  void *origin; /* typed buffer (read by pack, written by unpack) */
+  void *packed; /* contiguous bytes of this region */
+  tempi_desc desc;
+  int64_t incount;
+} tempi_region;
+
+typedef struct tempi_batch tempi_batch; /* opaque */
+
+int tempi_batch_create(const tempi_region *regions, int32_t n, int32_t unpack,
+                       tempi_batch **out);
+int tempi_batch_launch(tempi_batch *b, void *stream);
+/* capture one launch into a CUDA graph and replay it with tempi_batch_replay */
+int tempi_batch_capture(tempi_batch *b, void *stream);
+int tempi_batch_replay(tempi_batch *b, void *stream);
+int tempi_batch_destroy(tempi_batch *b);
+
+/* ---- runtime ------------------------------------------------------------ */
+/* TEMPI's internal non-blocking stream (a cudaStream_t) on which the MPI
+   entry points launch (reference kernStream, src/internal/streams.cpp:16-28).
+   Exposed so callers can order or time work against it. */
+void *tempi_stream(void);
+/* re-read the TEMPI_* environment knobs (MPI_Init reads them once) */
+int tempi_reload_env(void);
+
+/* ---- diagnostics -------------------------------------------------------- */
+const char *tempi_last_error(void);
+/* number of kernel launches issued by this library since load */
+int64_t tempi_kernel_launches(void);
+/* name of the kernel variant the last tempi_pack/unpack used */
+const char *tempi_last_kernel(void);
+/* value of a named counter (reference include/counters.hpp groups):
+   "packs", "unpacks", "lib_pack", "lib_unpack", "cached_types",
+   "send_device", "send_oneshot", "send_staged", "send_lib",
+   "recv_device", "recv_oneshot", "recv_staged", "recv_lib",
+   "isend_managed", "irecv_managed", "slab_hits", "slab_misses",
+   "dispatch_hit", "dispatch_miss"; -1 for an unknown name */
+int64_t tempi_counter(const char *name);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TEMPI_B200_H */

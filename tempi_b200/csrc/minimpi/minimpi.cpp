@@ -1,0 +1,1223 @@
+// libminimpi: a self-only MPI library (world size 1) that stands in for the
+// system MPI, which does not exist on the machines this project runs on.
+//
+// Datatypes follow the MPI-3.1 type-map definitions (section 4.1): each
+// constructor describes a sequence of (displacement, basic type) entries in a
+// fixed order, and MPI_Pack copies the described bytes in exactly that order.
+// The walker below visits that order, merging byte runs that are adjacent in
+// the source so that each merged run is one memcpy.
+//
+// Point-to-point calls match in MPI order: a send goes to the earliest posted
+// receive that matches it, else it is buffered (eagerly, always) as an
+// unexpected message; a receive takes the earliest matching unexpected message.
+// With one rank and one thread, a blocking receive that has nothing to match
+// can never complete, so it returns MPI_ERR_OTHER instead of hanging.
+
+#include "mpi.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <deque>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+
+struct TypeRec {
+  int combiner = MPI_COMBINER_NAMED;
+  std::vector<int> ints;
+  std::vector<MPI_Aint> addrs;
+  std::vector<MPI_Datatype> types;
+  int64_t size = 0;
+  int64_t lb = 0, ub = 0;           // extent = ub - lb
+  int64_t true_lb = 0, true_ub = 0; // bounds of the bytes actually described
+  bool dense = false; // type map is one ascending contiguous run, lb==true_lb
+  bool committed = false;
+  bool freed = false;
+  int64_t extent() const { return ub - lb; }
+};
+
+std::recursive_mutex g_mu;
+std::vector<TypeRec> g_types;
+bool g_initialized = false, g_finalized = false;
+
+void init_named() {
+  if (!g_types.empty())
+    return;
+  g_types.resize(MPI_UINT64_T + 1);
+  const int sizes[] = {0, 1, 1, 1, 2, 4, 4, 8, 8, 4, 8, 1, 8, 8};
+  for (int h = 1; h <= MPI_UINT64_T; ++h) {
+    TypeRec &t = g_types[h];
+    t.combiner = MPI_COMBINER_NAMED;
+    t.size = sizes[h];
+    t.lb = t.true_lb = 0;
+    t.ub = t.true_ub = sizes[h];
+    t.dense = true;
+    t.committed = true;
+  }
+}
+
+TypeRec *get(MPI_Datatype h) {
+  init_named();
+  if (h <= 0 || h >= (int)g_types.size() || g_types[h].freed)
+    return nullptr;
+  return &g_types[h];
+}
+
+MPI_Datatype add(TypeRec &&t) {
+  init_named();
+  g_types.push_back(std::move(t));
+  return (MPI_Datatype)(g_types.size() - 1);
+}
+
+// Bounds of a set of copies of child `c` placed at displacements in
+// [dmin, dmax] (both attained); `n` copies in total.
+void set_bounds(TypeRec &t, const TypeRec &c, int64_t dmin, int64_t dmax,
+                int64_t n) {
+  if (n <= 0 || (c.size == 0 && c.extent() == 0)) {
+    t.lb = t.ub = t.true_lb = t.true_ub = 0;
+    return;
+  }
+  t.lb = dmin + c.lb;
+  t.ub = dmax + c.ub;
+  t.true_lb = dmin + c.true_lb;
+  t.true_ub = dmax + c.true_ub;
+}
+
+// Range of j*step for 0 <= j < count.
+void term_range(int64_t count, int64_t step, int64_t &lo, int64_t &hi) {
+  int64_t last = (count - 1) * step;
+  lo = std::min<int64_t>(0, last);
+  hi = std::max<int64_t>(0, last);
+}
+
+// ---- type-map walk ---------------------------------------------------------
+
+struct Runs {
+  int64_t off = 0, len = 0;
+  template <class Flush> void emit(int64_t o, int64_t l, Flush &flush) {
+    if (l <= 0)
+      return;
+    if (len > 0 && o == off + len) {
+      len += l;
+      return;
+    }
+    if (len > 0)
+      flush(off, len);
+    off = o;
+    len = l;
+  }
+  template <class Flush> void finish(Flush &flush) {
+    if (len > 0)
+      flush(off, len);
+    len = 0;
+  }
+};
+
+template <class Flush>
+void walk(const TypeRec &t, int64_t base, Runs &r, Flush &flush);
+
+// `count` copies of child c, copy k at base + k*step
+template <class Flush>
+void walk_run(const TypeRec &c, int64_t base, int64_t count, int64_t step,
+              Runs &r, Flush &flush) {
+  if (c.dense && step == c.size) {
+    r.emit(base + c.lb, count * c.size, flush);
+    return;
+  }
+  for (int64_t k = 0; k < count; ++k)
+    walk(c, base + k * step, r, flush);
+}
+
+template <class Flush>
+void walk(const TypeRec &t, int64_t base, Runs &r, Flush &flush) {
+  if (t.dense) {
+    r.emit(base + t.true_lb, t.size, flush);
+    return;
+  }
+  switch (t.combiner) {
+  case MPI_COMBINER_DUP:
+  case MPI_COMBINER_RESIZED:
+    walk(g_types[t.types[0]], base, r, flush);
+    return;
+  case MPI_COMBINER_CONTIGUOUS: {
+    const TypeRec &c = g_types[t.types[0]];
+    walk_run(c, base, t.ints[0], c.extent(), r, flush);
+    return;
+  }
+  case MPI_COMBINER_VECTOR:
+  case MPI_COMBINER_HVECTOR: {
+    const TypeRec &c = g_types[t.types[0]];
+    const int64_t count = t.ints[0], bl = t.ints[1];
+    const int64_t stride = t.combiner == MPI_COMBINER_VECTOR
+                               ? int64_t(t.ints[2]) * c.extent()
+                               : int64_t(t.addrs[0]);
+    for (int64_t j = 0; j < count; ++j)
+      walk_run(c, base + j * stride, bl, c.extent(), r, flush);
+    return;
+  }
+  case MPI_COMBINER_INDEXED:
+  case MPI_COMBINER_HINDEXED: {
+    const TypeRec &c = g_types[t.types[0]];
+    const int n = t.ints[0];
+    for (int i = 0; i < n; ++i) {
+      int64_t d = t.combiner == MPI_COMBINER_INDEXED
+                      ? int64_t(t.ints[1 + n + i]) * c.extent()
+                      : int64_t(t.addrs[i]);
+      walk_run(c, base + d, t.ints[1 + i], c.extent(), r, flush);
+    }
+    return;
+  }
+  case MPI_COMBINER_INDEXED_BLOCK:
+  case MPI_COMBINER_HINDEXED_BLOCK: {
+    const TypeRec &c = g_types[t.types[0]];
+    const int n = t.ints[0], bl = t.ints[1];
+    for (int i = 0; i < n; ++i) {
+      int64_t d = t.combiner == MPI_COMBINER_INDEXED_BLOCK
+                      ? int64_t(t.ints[2 + i]) * c.extent()
+                      : int64_t(t.addrs[i]);
+      walk_run(c, base + d, bl, c.extent(), r, flush);
+    }
+    return;
+  }
+  case MPI_COMBINER_STRUCT: {
+    const int n = t.ints[0];
+    for (int i = 0; i < n; ++i) {
+      const TypeRec &c = g_types[t.types[i]];
+      walk_run(c, base + t.addrs[i], t.ints[1 + i], c.extent(), r, flush);
+    }
+    return;
+  }
+  case MPI_COMBINER_SUBARRAY: {
+    const TypeRec &c = g_types[t.types[0]];
+    const int nd = t.ints[0];
+    const int *sizes = &t.ints[1], *subs = &t.ints[1 + nd],
+              *starts = &t.ints[1 + 2 * nd];
+    const bool corder = t.ints[1 + 3 * nd] == MPI_ORDER_C;
+    // dims listed slowest-varying first
+    std::vector<int64_t> cnt(nd), str(nd);
+    int64_t off = 0;
+    for (int k = 0; k < nd; ++k) {
+      int d = corder ? k : nd - 1 - k;
+      int64_t s = c.extent();
+      if (corder)
+        for (int j = d + 1; j < nd; ++j)
+          s *= sizes[j];
+      else
+        for (int j = 0; j < d; ++j)
+          s *= sizes[j];
+      cnt[k] = subs[d];
+      str[k] = s;
+      off += int64_t(starts[d]) * s;
+    }
+    for (int k = 0; k < nd; ++k)
+      if (cnt[k] == 0)
+        return;
+    std::vector<int64_t> idx(nd, 0);
+    const int inner = nd - 1;
+    while (true) {
+      int64_t o = base + off;
+      for (int k = 0; k < inner; ++k)
+        o += idx[k] * str[k];
+      walk_run(c, o, cnt[inner], str[inner], r, flush);
+      int k = inner - 1;
+      while (k >= 0 && ++idx[k] == cnt[k]) {
+        idx[k] = 0;
+        --k;
+      }
+      if (k < 0)
+        break;
+    }
+    return;
+  }
+  default:
+    return;
+  }
+}
+
+// ---- device awareness ------------------------------------------------------
+
+bool is_device(const void *p) {
+  if (!p)
+    return false;
+  cudaPointerAttributes a{};
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice;
+}
+
+// byte span [lo, hi) touched by `count` objects of type t
+void span(const TypeRec &t, int64_t count, int64_t &lo, int64_t &hi) {
+  if (count <= 0 || t.size == 0) {
+    lo = hi = 0;
+    return;
+  }
+  int64_t a = 0, b = (count - 1) * t.extent();
+  lo = std::min(a, b) + t.true_lb;
+  hi = std::max(a, b) + t.true_ub;
+}
+
+// pack `count` objects at `in` (host memory) into `out` (host memory)
+int64_t pack_host(const TypeRec &t, const char *in, int64_t count, char *out) {
+  int64_t pos = 0;
+  auto flush = [&](int64_t o, int64_t l) {
+    std::memcpy(out + pos, in + o, l);
+    pos += l;
+  };
+  Runs r;
+  for (int64_t i = 0; i < count; ++i)
+    walk(t, i * t.extent(), r, flush);
+  r.finish(flush);
+  return pos;
+}
+
+int64_t unpack_host(const TypeRec &t, const char *in, int64_t count,
+                    char *out) {
+  int64_t pos = 0;
+  auto flush = [&](int64_t o, int64_t l) {
+    std::memcpy(out + o, in + pos, l);
+    pos += l;
+  };
+  Runs r;
+  for (int64_t i = 0; i < count; ++i)
+    walk(t, i * t.extent(), r, flush);
+  r.finish(flush);
+  return pos;
+}
+
+// pack from any memory into a host vector
+int pack_any(const TypeRec &t, const void *buf, int64_t count,
+             std::vector<char> &out) {
+  out.resize(size_t(count * t.size));
+  if (out.empty())
+    return MPI_SUCCESS;
+  if (!is_device(buf)) {
+    pack_host(t, (const char *)buf, count, out.data());
+    return MPI_SUCCESS;
+  }
+  int64_t lo, hi;
+  span(t, count, lo, hi);
+  std::vector<char> stage(size_t(hi - lo));
+  if (cudaMemcpy(stage.data(), (const char *)buf + lo, hi - lo,
+                 cudaMemcpyDefault) != cudaSuccess)
+    return MPI_ERR_OTHER;
+  pack_host(t, stage.data() - lo, count, out.data());
+  return MPI_SUCCESS;
+}
+
+// unpack `n` packed bytes into any memory
+int unpack_any(const TypeRec &t, const char *packed, int64_t count, void *buf) {
+  if (count <= 0 || t.size == 0)
+    return MPI_SUCCESS;
+  if (!is_device(buf)) {
+    unpack_host(t, packed, count, (char *)buf);
+    return MPI_SUCCESS;
+  }
+  int64_t lo, hi;
+  span(t, count, lo, hi);
+  std::vector<char> stage(size_t(hi - lo));
+  char *dev = (char *)buf + lo;
+  if (cudaMemcpy(stage.data(), dev, hi - lo, cudaMemcpyDefault) != cudaSuccess)
+    return MPI_ERR_OTHER;
+  unpack_host(t, packed, count, stage.data() - lo);
+  if (cudaMemcpy(dev, stage.data(), hi - lo, cudaMemcpyDefault) != cudaSuccess)
+    return MPI_ERR_OTHER;
+  return MPI_SUCCESS;
+}
+
+// ---- point to point ----------------------------------------------------------
+
+// A buffered message.  Contiguous payloads sent from device memory stay in
+// device memory (a CUDA-aware MPI moves them device to device); everything
+// else is packed into host memory.
+struct Message {
+  int tag;
+  MPI_Comm comm;
+  std::vector<char> data; // host payload
+  void *dev = nullptr;    // device payload, if any
+  int64_t bytes = 0;
+};
+
+std::unordered_map<int64_t, std::vector<void *>> g_dev_pool;
+
+void *dev_get(int64_t n) {
+  auto &v = g_dev_pool[n];
+  if (!v.empty()) {
+    void *p = v.back();
+    v.pop_back();
+    return p;
+  }
+  void *p = nullptr;
+  if (cudaMalloc(&p, n) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void dev_put(void *p, int64_t n) {
+  if (p)
+    g_dev_pool[n].push_back(p);
+}
+
+struct Req {
+  bool send = false, persistent = false, active = false, complete = false;
+  const void *sbuf = nullptr;
+  void *rbuf = nullptr;
+  int count = 0;
+  MPI_Datatype type = MPI_DATATYPE_NULL;
+  int peer = 0, tag = 0;
+  MPI_Comm comm = MPI_COMM_WORLD;
+  MPI_Status st{};
+};
+
+std::deque<Message> g_unexpected;
+std::deque<int> g_posted; // active receive requests, in posting order
+std::unordered_map<int, Req> g_reqs;
+int g_next_req = 1;
+
+bool valid_comm(MPI_Comm c) { return c == MPI_COMM_WORLD || c == MPI_COMM_SELF; }
+
+bool tag_match(int want, int have) { return want == MPI_ANY_TAG || want == have; }
+
+// deliver message bytes into a receive request
+int deliver(Req &r, const Message &m) {
+  const TypeRec *t = get(r.type);
+  if (!t)
+    return MPI_ERR_TYPE;
+  int64_t cap = int64_t(r.count) * t->size;
+  int64_t n = m.bytes;
+  int err = MPI_SUCCESS;
+  if (n > cap) {
+    err = MPI_ERR_TRUNCATE;
+    n = cap;
+  }
+  int64_t whole = t->size ? n / t->size : 0;
+  int e2 = MPI_SUCCESS;
+  if (t->dense && n > 0) {
+    // contiguous receive: one copy, whatever memory either side is in
+    char *dst = (char *)r.rbuf + t->lb;
+    const void *src = m.dev ? m.dev : (const void *)m.data.data();
+    if (!m.dev && !is_device(r.rbuf))
+      std::memcpy(dst, src, n);
+    else if (cudaMemcpy(dst, src, n, cudaMemcpyDefault) != cudaSuccess)
+      e2 = MPI_ERR_OTHER;
+  } else if (m.dev) {
+    std::vector<char> host(size_t(m.bytes));
+    if (cudaMemcpy(host.data(), m.dev, m.bytes, cudaMemcpyDefault) !=
+        cudaSuccess)
+      e2 = MPI_ERR_OTHER;
+    else
+      e2 = unpack_any(*t, host.data(), whole, r.rbuf);
+  } else {
+    e2 = unpack_any(*t, m.data.data(), whole, r.rbuf);
+  }
+  if (e2 != MPI_SUCCESS)
+    err = e2;
+  r.st.MPI_SOURCE = 0;
+  r.st.MPI_TAG = m.tag;
+  r.st.MPI_ERROR = err;
+  r.st.bytes_ = n;
+  r.complete = true;
+  return err;
+}
+
+int do_send(const void *buf, int count, MPI_Datatype type, int dest, int tag,
+            MPI_Comm comm) {
+  if (!valid_comm(comm))
+    return MPI_ERR_COMM;
+  if (dest == MPI_PROC_NULL)
+    return MPI_SUCCESS;
+  if (dest != 0)
+    return MPI_ERR_RANK;
+  if (count < 0)
+    return MPI_ERR_COUNT;
+  const TypeRec *t = get(type);
+  if (!t)
+    return MPI_ERR_TYPE;
+  Message m{tag, comm, {}, nullptr, int64_t(count) * t->size};
+  if (t->dense && m.bytes > 0 && is_device(buf)) {
+    m.dev = dev_get(m.bytes);
+    if (!m.dev || cudaMemcpy(m.dev, (const char *)buf + t->lb, m.bytes,
+                             cudaMemcpyDefault) != cudaSuccess)
+      return MPI_ERR_OTHER;
+  } else {
+    int err = pack_any(*t, buf, count, m.data);
+    if (err)
+      return err;
+  }
+  for (auto it = g_posted.begin(); it != g_posted.end(); ++it) {
+    Req &r = g_reqs[*it];
+    if (r.comm == comm && (r.peer == 0 || r.peer == MPI_ANY_SOURCE) &&
+        tag_match(r.tag, tag)) {
+      g_posted.erase(it);
+      deliver(r, m);
+      dev_put(m.dev, m.bytes);
+      return MPI_SUCCESS;
+    }
+  }
+  g_unexpected.push_back(std::move(m));
+  return MPI_SUCCESS;
+}
+
+// try to satisfy an active receive from the unexpected queue
+bool try_match(Req &r) {
+  for (auto it = g_unexpected.begin(); it != g_unexpected.end(); ++it) {
+    if (it->comm == r.comm && tag_match(r.tag, it->tag)) {
+      Message m = std::move(*it);
+      g_unexpected.erase(it);
+      deliver(r, m);
+      dev_put(m.dev, m.bytes);
+      return true;
+    }
+  }
+  return false;
+}
+
+int start_req(int id) {
+  Req &r = g_reqs[id];
+  r.active = true;
+  r.complete = false;
+  r.st = MPI_Status{};
+  if (r.send) {
+    int err = do_send(r.sbuf, r.count, r.type, r.peer, r.tag, r.comm);
+    r.complete = true;
+    r.st.MPI_ERROR = err;
+    return err;
+  }
+  if (r.peer == MPI_PROC_NULL) {
+    r.complete = true;
+    r.st.MPI_SOURCE = MPI_PROC_NULL;
+    r.st.MPI_TAG = MPI_ANY_TAG;
+    return MPI_SUCCESS;
+  }
+  if (r.peer != 0 && r.peer != MPI_ANY_SOURCE)
+    return MPI_ERR_RANK;
+  if (!try_match(r))
+    g_posted.push_back(id);
+  return MPI_SUCCESS;
+}
+
+int new_req(Req &&r) {
+  int id = g_next_req++;
+  if (g_next_req >= 0x40000000)
+    g_next_req = 1; // stay clear of the high bit range
+  g_reqs[id] = std::move(r);
+  return id;
+}
+
+void finish_req(MPI_Request *request, MPI_Status *status) {
+  Req &r = g_reqs[*request];
+  if (status)
+    *status = r.st;
+  if (r.persistent) {
+    r.active = false;
+  } else {
+    g_reqs.erase(*request);
+    *request = MPI_REQUEST_NULL;
+  }
+}
+
+int new_type(TypeRec &&t, MPI_Datatype *newtype) {
+  if (!newtype)
+    return MPI_ERR_ARG;
+  *newtype = add(std::move(t));
+  return MPI_SUCCESS;
+}
+
+} // namespace
+
+extern "C" {
+
+int MPI_Init(int *, char ***) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  init_named();
+  g_initialized = true;
+  return MPI_SUCCESS;
+}
+int MPI_Init_thread(int *argc, char ***argv, int required, int *provided) {
+  (void)required;
+  if (provided)
+    *provided = MPI_THREAD_SERIALIZED;
+  return MPI_Init(argc, argv);
+}
+int MPI_Finalize(void) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  g_finalized = true;
+  return MPI_SUCCESS;
+}
+int MPI_Initialized(int *flag) {
+  *flag = g_initialized;
+  return MPI_SUCCESS;
+}
+int MPI_Finalized(int *flag) {
+  *flag = g_finalized;
+  return MPI_SUCCESS;
+}
+int MPI_Abort(MPI_Comm, int errorcode) {
+  std::fprintf(stderr, "minimpi: MPI_Abort(%d)\n", errorcode);
+  std::exit(errorcode);
+}
+double MPI_Wtime(void) {
+  timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+int MPI_Get_library_version(char *version, int *resultlen) {
+  const char *s = "minimpi 1.0 (self-only MPI stand-in)";
+  std::strncpy(version, s, MPI_MAX_LIBRARY_VERSION_STRING - 1);
+  version[MPI_MAX_LIBRARY_VERSION_STRING - 1] = 0;
+  *resultlen = (int)std::strlen(version);
+  return MPI_SUCCESS;
+}
+int MPI_Comm_rank(MPI_Comm comm, int *rank) {
+  if (!valid_comm(comm))
+    return MPI_ERR_COMM;
+  *rank = 0;
+  return MPI_SUCCESS;
+}
+int MPI_Comm_size(MPI_Comm comm, int *size) {
+  if (!valid_comm(comm))
+    return MPI_ERR_COMM;
+  *size = 1;
+  return MPI_SUCCESS;
+}
+int MPI_Barrier(MPI_Comm comm) {
+  return valid_comm(comm) ? MPI_SUCCESS : MPI_ERR_COMM;
+}
+int MPI_Error_string(int errorcode, char *string, int *resultlen) {
+  std::snprintf(string, 64, "MPI error %d", errorcode);
+  *resultlen = (int)std::strlen(string);
+  return MPI_SUCCESS;
+}
+
+int MPI_Type_contiguous(int count, MPI_Datatype oldtype,
+                        MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *c = get(oldtype);
+  if (!c)
+    return MPI_ERR_TYPE;
+  if (count < 0)
+    return MPI_ERR_COUNT;
+  TypeRec t;
+  t.combiner = MPI_COMBINER_CONTIGUOUS;
+  t.ints = {count};
+  t.types = {oldtype};
+  t.size = count * c->size;
+  int64_t lo, hi;
+  term_range(count, c->extent(), lo, hi);
+  set_bounds(t, *c, lo, hi, count);
+  t.dense = c->dense && count > 0;
+  return new_type(std::move(t), newtype);
+}
+
+static int make_vector(int combiner, int count, int bl, int64_t stride_bytes,
+                       const std::vector<int> &ints,
+                       const std::vector<MPI_Aint> &addrs, MPI_Datatype oldtype,
+                       MPI_Datatype *newtype) {
+  const TypeRec *c = get(oldtype);
+  if (!c)
+    return MPI_ERR_TYPE;
+  if (count < 0 || bl < 0)
+    return MPI_ERR_COUNT;
+  TypeRec t;
+  t.combiner = combiner;
+  t.ints = ints;
+  t.addrs = addrs;
+  t.types = {oldtype};
+  t.size = int64_t(count) * bl * c->size;
+  int64_t a0, a1, b0, b1;
+  term_range(count, stride_bytes, a0, a1);
+  term_range(bl, c->extent(), b0, b1);
+  set_bounds(t, *c, a0 + b0, a1 + b1, int64_t(count) * bl);
+  t.dense = c->dense && count > 0 && bl > 0 &&
+            (count == 1 || stride_bytes == bl * c->extent());
+  return new_type(std::move(t), newtype);
+}
+
+int MPI_Type_vector(int count, int blocklength, int stride,
+                    MPI_Datatype oldtype, MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *c = get(oldtype);
+  if (!c)
+    return MPI_ERR_TYPE;
+  return make_vector(MPI_COMBINER_VECTOR, count, blocklength,
+                     int64_t(stride) * c->extent(),
+                     {count, blocklength, stride}, {}, oldtype, newtype);
+}
+
+int MPI_Type_create_hvector(int count, int blocklength, MPI_Aint stride,
+                            MPI_Datatype oldtype, MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  return make_vector(MPI_COMBINER_HVECTOR, count, blocklength, stride,
+                     {count, blocklength}, {stride}, oldtype, newtype);
+}
+
+// blocks of bls[i] copies of c at byte displacements d[i]
+static void bounds_blocks(TypeRec &t, const TypeRec &c,
+                          const std::vector<int64_t> &bl,
+                          const std::vector<int64_t> &d) {
+  bool any = false;
+  int64_t lb = 0, ub = 0, tlb = 0, tub = 0;
+  for (size_t i = 0; i < bl.size(); ++i) {
+    if (bl[i] <= 0)
+      continue;
+    int64_t lo, hi;
+    term_range(bl[i], c.extent(), lo, hi);
+    int64_t l0 = d[i] + lo + c.lb, u0 = d[i] + hi + c.ub;
+    int64_t tl = d[i] + lo + c.true_lb, tu = d[i] + hi + c.true_ub;
+    if (!any) {
+      lb = l0, ub = u0, tlb = tl, tub = tu, any = true;
+    } else {
+      lb = std::min(lb, l0), ub = std::max(ub, u0);
+      tlb = std::min(tlb, tl), tub = std::max(tub, tu);
+    }
+  }
+  t.lb = lb, t.ub = ub, t.true_lb = tlb, t.true_ub = tub;
+}
+
+int MPI_Type_indexed(int count, const int bls[], const int displs[],
+                     MPI_Datatype oldtype, MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *c = get(oldtype);
+  if (!c)
+    return MPI_ERR_TYPE;
+  if (count < 0)
+    return MPI_ERR_COUNT;
+  TypeRec t;
+  t.combiner = MPI_COMBINER_INDEXED;
+  t.ints.push_back(count);
+  std::vector<int64_t> bl, d;
+  for (int i = 0; i < count; ++i)
+    t.ints.push_back(bls[i]), bl.push_back(bls[i]), t.size += bls[i] * c->size;
+  for (int i = 0; i < count; ++i)
+    t.ints.push_back(displs[i]), d.push_back(int64_t(displs[i]) * c->extent());
+  t.types = {oldtype};
+  bounds_blocks(t, *c, bl, d);
+  return new_type(std::move(t), newtype);
+}
+
+int MPI_Type_create_hindexed(int count, const int bls[], const MPI_Aint displs[],
+                             MPI_Datatype oldtype, MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *c = get(oldtype);
+  if (!c)
+    return MPI_ERR_TYPE;
+  if (count < 0)
+    return MPI_ERR_COUNT;
+  TypeRec t;
+  t.combiner = MPI_COMBINER_HINDEXED;
+  t.ints.push_back(count);
+  std::vector<int64_t> bl, d;
+  for (int i = 0; i < count; ++i) {
+    t.ints.push_back(bls[i]);
+    t.addrs.push_back(displs[i]);
+    bl.push_back(bls[i]);
+    d.push_back(displs[i]);
+    t.size += bls[i] * c->size;
+  }
+  t.types = {oldtype};
+  bounds_blocks(t, *c, bl, d);
+  return new_type(std::move(t), newtype);
+}
+
+int MPI_Type_create_indexed_block(int count, int blocklength,
+                                  const int displs[], MPI_Datatype oldtype,
+                                  MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *c = get(oldtype);
+  if (!c)
+    return MPI_ERR_TYPE;
+  if (count < 0 || blocklength < 0)
+    return MPI_ERR_COUNT;
+  TypeRec t;
+  t.combiner = MPI_COMBINER_INDEXED_BLOCK;
+  t.ints = {count, blocklength};
+  std::vector<int64_t> bl(count, blocklength), d;
+  for (int i = 0; i < count; ++i)
+    t.ints.push_back(displs[i]), d.push_back(int64_t(displs[i]) * c->extent());
+  t.types = {oldtype};
+  t.size = int64_t(count) * blocklength * c->size;
+  bounds_blocks(t, *c, bl, d);
+  return new_type(std::move(t), newtype);
+}
+
+int MPI_Type_create_hindexed_block(int count, int blocklength,
+                                   const MPI_Aint displs[],
+                                   MPI_Datatype oldtype,
+                                   MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *c = get(oldtype);
+  if (!c)
+    return MPI_ERR_TYPE;
+  if (count < 0 || blocklength < 0)
+    return MPI_ERR_COUNT;
+  TypeRec t;
+  t.combiner = MPI_COMBINER_HINDEXED_BLOCK;
+  t.ints = {count, blocklength};
+  std::vector<int64_t> bl(count, blocklength), d;
+  for (int i = 0; i < count; ++i)
+    t.addrs.push_back(displs[i]), d.push_back(displs[i]);
+  t.types = {oldtype};
+  t.size = int64_t(count) * blocklength * c->size;
+  bounds_blocks(t, *c, bl, d);
+  return new_type(std::move(t), newtype);
+}
+
+int MPI_Type_create_struct(int count, const int bls[], const MPI_Aint displs[],
+                           const MPI_Datatype types[], MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (count < 0)
+    return MPI_ERR_COUNT;
+  TypeRec t;
+  t.combiner = MPI_COMBINER_STRUCT;
+  t.ints.push_back(count);
+  bool any = false;
+  for (int i = 0; i < count; ++i) {
+    const TypeRec *c = get(types[i]);
+    if (!c)
+      return MPI_ERR_TYPE;
+    t.ints.push_back(bls[i]);
+    t.addrs.push_back(displs[i]);
+    t.types.push_back(types[i]);
+    t.size += bls[i] * c->size;
+    if (bls[i] <= 0)
+      continue;
+    TypeRec one;
+    bounds_blocks(one, *c, {bls[i]}, {displs[i]});
+    if (!any) {
+      t.lb = one.lb, t.ub = one.ub, t.true_lb = one.true_lb,
+      t.true_ub = one.true_ub, any = true;
+    } else {
+      t.lb = std::min(t.lb, one.lb), t.ub = std::max(t.ub, one.ub);
+      t.true_lb = std::min(t.true_lb, one.true_lb);
+      t.true_ub = std::max(t.true_ub, one.true_ub);
+    }
+  }
+  return new_type(std::move(t), newtype);
+}
+
+int MPI_Type_create_subarray(int ndims, const int sizes[], const int subsizes[],
+                             const int starts[], int order,
+                             MPI_Datatype oldtype, MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *c = get(oldtype);
+  if (!c)
+    return MPI_ERR_TYPE;
+  if (ndims <= 0 || (order != MPI_ORDER_C && order != MPI_ORDER_FORTRAN))
+    return MPI_ERR_ARG;
+  for (int d = 0; d < ndims; ++d)
+    if (sizes[d] <= 0 || subsizes[d] < 0 || starts[d] < 0 ||
+        starts[d] + subsizes[d] > sizes[d])
+      return MPI_ERR_ARG;
+  TypeRec t;
+  t.combiner = MPI_COMBINER_SUBARRAY;
+  t.ints.push_back(ndims);
+  for (int d = 0; d < ndims; ++d)
+    t.ints.push_back(sizes[d]);
+  for (int d = 0; d < ndims; ++d)
+    t.ints.push_back(subsizes[d]);
+  for (int d = 0; d < ndims; ++d)
+    t.ints.push_back(starts[d]);
+  t.ints.push_back(order);
+  t.types = {oldtype};
+  int64_t n = 1, full = 1;
+  bool whole = true;
+  int64_t tlo = 0, thi = 0;
+  for (int d = 0; d < ndims; ++d) {
+    n *= subsizes[d];
+    full *= sizes[d];
+    whole = whole && subsizes[d] == sizes[d];
+  }
+  // true bounds: first and last described element
+  int64_t first = 0, last = 0;
+  for (int d = 0; d < ndims; ++d) {
+    int64_t s = c->extent();
+    if (order == MPI_ORDER_C)
+      for (int j = d + 1; j < ndims; ++j)
+        s *= sizes[j];
+    else
+      for (int j = 0; j < d; ++j)
+        s *= sizes[j];
+    first += int64_t(starts[d]) * s;
+    last += int64_t(starts[d] + subsizes[d] - 1) * s;
+  }
+  tlo = first + c->true_lb;
+  thi = last + c->true_ub;
+  t.size = n * c->size;
+  // the subarray type spans the whole array: lb = 0, extent = prod(sizes)*ext
+  t.lb = 0;
+  t.ub = full * c->extent();
+  if (n > 0) {
+    t.true_lb = tlo;
+    t.true_ub = thi;
+  }
+  t.dense = c->dense && whole;
+  return new_type(std::move(t), newtype);
+}
+
+int MPI_Type_create_resized(MPI_Datatype oldtype, MPI_Aint lb, MPI_Aint extent,
+                            MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *c = get(oldtype);
+  if (!c)
+    return MPI_ERR_TYPE;
+  TypeRec t;
+  t.combiner = MPI_COMBINER_RESIZED;
+  t.addrs = {lb, extent};
+  t.types = {oldtype};
+  t.size = c->size;
+  t.lb = lb;
+  t.ub = lb + extent;
+  t.true_lb = c->true_lb;
+  t.true_ub = c->true_ub;
+  t.dense = c->dense && lb == c->lb && extent == c->extent();
+  return new_type(std::move(t), newtype);
+}
+
+int MPI_Type_dup(MPI_Datatype oldtype, MPI_Datatype *newtype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *c = get(oldtype);
+  if (!c)
+    return MPI_ERR_TYPE;
+  TypeRec t = *c;
+  t.combiner = MPI_COMBINER_DUP;
+  t.ints.clear();
+  t.addrs.clear();
+  t.types = {oldtype};
+  t.committed = false;
+  return new_type(std::move(t), newtype);
+}
+
+int MPI_Type_commit(MPI_Datatype *datatype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  TypeRec *t = get(datatype ? *datatype : 0);
+  if (!t)
+    return MPI_ERR_TYPE;
+  t->committed = true;
+  return MPI_SUCCESS;
+}
+
+int MPI_Type_free(MPI_Datatype *datatype) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  TypeRec *t = get(datatype ? *datatype : 0);
+  if (!t || t->combiner == MPI_COMBINER_NAMED)
+    return MPI_ERR_TYPE;
+  // handles are never reused, so types built on this one stay valid
+  t->freed = true;
+  *datatype = MPI_DATATYPE_NULL;
+  return MPI_SUCCESS;
+}
+
+int MPI_Type_size(MPI_Datatype datatype, int *size) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *t = get(datatype);
+  if (!t)
+    return MPI_ERR_TYPE;
+  *size = (int)t->size;
+  return MPI_SUCCESS;
+}
+
+int MPI_Type_get_extent(MPI_Datatype datatype, MPI_Aint *lb, MPI_Aint *extent) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *t = get(datatype);
+  if (!t)
+    return MPI_ERR_TYPE;
+  *lb = t->lb;
+  *extent = t->extent();
+  return MPI_SUCCESS;
+}
+
+int MPI_Type_get_true_extent(MPI_Datatype datatype, MPI_Aint *true_lb,
+                             MPI_Aint *true_extent) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *t = get(datatype);
+  if (!t)
+    return MPI_ERR_TYPE;
+  *true_lb = t->true_lb;
+  *true_extent = t->true_ub - t->true_lb;
+  return MPI_SUCCESS;
+}
+
+int MPI_Type_get_envelope(MPI_Datatype datatype, int *ni, int *na, int *nd,
+                          int *combiner) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *t = get(datatype);
+  if (!t)
+    return MPI_ERR_TYPE;
+  *combiner = t->combiner;
+  if (t->combiner == MPI_COMBINER_NAMED) {
+    *ni = *na = *nd = 0;
+  } else {
+    *ni = (int)t->ints.size();
+    *na = (int)t->addrs.size();
+    *nd = (int)t->types.size();
+  }
+  return MPI_SUCCESS;
+}
+
+int MPI_Type_get_contents(MPI_Datatype datatype, int max_integers,
+                          int max_addresses, int max_datatypes, int ints[],
+                          MPI_Aint addrs[], MPI_Datatype types[]) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *t = get(datatype);
+  if (!t || t->combiner == MPI_COMBINER_NAMED)
+    return MPI_ERR_TYPE;
+  if (max_integers < (int)t->ints.size() ||
+      max_addresses < (int)t->addrs.size() ||
+      max_datatypes < (int)t->types.size())
+    return MPI_ERR_ARG;
+  std::copy(t->ints.begin(), t->ints.end(), ints);
+  std::copy(t->addrs.begin(), t->addrs.end(), addrs);
+  std::copy(t->types.begin(), t->types.end(), types);
+  return MPI_SUCCESS;
+}
+
+int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
+             void *outbuf, int outsize, int *position, MPI_Comm comm) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!valid_comm(comm))
+    return MPI_ERR_COMM;
+  const TypeRec *t = get(datatype);
+  if (!t)
+    return MPI_ERR_TYPE;
+  if (incount < 0 || !position || *position < 0)
+    return MPI_ERR_ARG;
+  int64_t need = int64_t(incount) * t->size;
+  if (*position + need > outsize)
+    return MPI_ERR_TRUNCATE;
+  std::vector<char> packed;
+  int err = pack_any(*t, inbuf, incount, packed);
+  if (err)
+    return err;
+  char *dst = (char *)outbuf + *position;
+  if (is_device(outbuf)) {
+    if (need && cudaMemcpy(dst, packed.data(), need, cudaMemcpyDefault) !=
+                    cudaSuccess)
+      return MPI_ERR_OTHER;
+  } else if (need) {
+    std::memcpy(dst, packed.data(), need);
+  }
+  *position += (int)need;
+  return MPI_SUCCESS;
+}
+
+int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
+               int outcount, MPI_Datatype datatype, MPI_Comm comm) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!valid_comm(comm))
+    return MPI_ERR_COMM;
+  const TypeRec *t = get(datatype);
+  if (!t)
+    return MPI_ERR_TYPE;
+  if (outcount < 0 || !position || *position < 0)
+    return MPI_ERR_ARG;
+  int64_t need = int64_t(outcount) * t->size;
+  if (*position + need > insize)
+    return MPI_ERR_TRUNCATE;
+  std::vector<char> packed((size_t)need);
+  const char *src = (const char *)inbuf + *position;
+  if (need) {
+    if (is_device(inbuf)) {
+      if (cudaMemcpy(packed.data(), src, need, cudaMemcpyDefault) !=
+          cudaSuccess)
+        return MPI_ERR_OTHER;
+    } else {
+      std::memcpy(packed.data(), src, need);
+    }
+  }
+  int err = unpack_any(*t, packed.data(), outcount, outbuf);
+  if (err)
+    return err;
+  *position += (int)need;
+  return MPI_SUCCESS;
+}
+
+int MPI_Pack_size(int incount, MPI_Datatype datatype, MPI_Comm comm,
+                  int *size) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!valid_comm(comm))
+    return MPI_ERR_COMM;
+  const TypeRec *t = get(datatype);
+  if (!t)
+    return MPI_ERR_TYPE;
+  *size = (int)(int64_t(incount) * t->size);
+  return MPI_SUCCESS;
+}
+
+int MPI_Send(const void *buf, int count, MPI_Datatype datatype, int dest,
+             int tag, MPI_Comm comm) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  return do_send(buf, count, datatype, dest, tag, comm);
+}
+
+int MPI_Recv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
+             MPI_Comm comm, MPI_Status *status) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  MPI_Request req;
+  int err = MPI_Irecv(buf, count, datatype, source, tag, comm, &req);
+  if (err)
+    return err;
+  err = MPI_Wait(&req, status);
+  if (err && req != MPI_REQUEST_NULL)
+    MPI_Request_free(&req);
+  return err;
+}
+
+int MPI_Isend(const void *buf, int count, MPI_Datatype datatype, int dest,
+              int tag, MPI_Comm comm, MPI_Request *request) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  int err = MPI_Send_init(buf, count, datatype, dest, tag, comm, request);
+  if (err)
+    return err;
+  g_reqs[*request].persistent = false;
+  return start_req(*request);
+}
+
+int MPI_Irecv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
+              MPI_Comm comm, MPI_Request *request) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  int err = MPI_Recv_init(buf, count, datatype, source, tag, comm, request);
+  if (err)
+    return err;
+  g_reqs[*request].persistent = false;
+  return start_req(*request);
+}
+
+int MPI_Send_init(const void *buf, int count, MPI_Datatype datatype, int dest,
+                  int tag, MPI_Comm comm, MPI_Request *request) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!valid_comm(comm))
+    return MPI_ERR_COMM;
+  if (!get(datatype))
+    return MPI_ERR_TYPE;
+  Req r;
+  r.send = true;
+  r.persistent = true;
+  r.sbuf = buf;
+  r.count = count;
+  r.type = datatype;
+  r.peer = dest;
+  r.tag = tag;
+  r.comm = comm;
+  *request = new_req(std::move(r));
+  return MPI_SUCCESS;
+}
+
+int MPI_Recv_init(void *buf, int count, MPI_Datatype datatype, int source,
+                  int tag, MPI_Comm comm, MPI_Request *request) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!valid_comm(comm))
+    return MPI_ERR_COMM;
+  if (!get(datatype))
+    return MPI_ERR_TYPE;
+  Req r;
+  r.send = false;
+  r.persistent = true;
+  r.rbuf = buf;
+  r.count = count;
+  r.type = datatype;
+  r.peer = source;
+  r.tag = tag;
+  r.comm = comm;
+  *request = new_req(std::move(r));
+  return MPI_SUCCESS;
+}
+
+int MPI_Start(MPI_Request *request) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!request || !g_reqs.count(*request))
+    return MPI_ERR_REQUEST;
+  Req &r = g_reqs[*request];
+  if (!r.persistent || r.active)
+    return MPI_ERR_REQUEST;
+  return start_req(*request);
+}
+
+int MPI_Test(MPI_Request *request, int *flag, MPI_Status *status) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!request)
+    return MPI_ERR_REQUEST;
+  if (*request == MPI_REQUEST_NULL) {
+    *flag = 1;
+    return MPI_SUCCESS;
+  }
+  auto it = g_reqs.find(*request);
+  if (it == g_reqs.end())
+    return MPI_ERR_REQUEST;
+  Req &r = it->second;
+  if (r.persistent && !r.active) {
+    *flag = 1;
+    return MPI_SUCCESS;
+  }
+  *flag = r.complete;
+  if (!r.complete)
+    return MPI_SUCCESS;
+  int err = r.st.MPI_ERROR;
+  finish_req(request, status);
+  return err;
+}
+
+int MPI_Wait(MPI_Request *request, MPI_Status *status) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  int flag = 0;
+  int err = MPI_Test(request, &flag, status);
+  if (err)
+    return err;
+  if (!flag) {
+    // one rank, one thread: no send can arrive while we block
+    std::fprintf(stderr,
+                 "minimpi: MPI_Wait on a receive with no matching send "
+                 "(would deadlock at world size 1)\n");
+    return MPI_ERR_OTHER;
+  }
+  return MPI_SUCCESS;
+}
+
+int MPI_Waitall(int count, MPI_Request reqs[], MPI_Status stats[]) {
+  int err = MPI_SUCCESS;
+  for (int i = 0; i < count; ++i) {
+    int e = MPI_Wait(&reqs[i], stats ? &stats[i] : MPI_STATUS_IGNORE);
+    if (e && !err)
+      err = e;
+  }
+  return err;
+}
+
+int MPI_Request_free(MPI_Request *request) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!request || !g_reqs.count(*request))
+    return MPI_ERR_REQUEST;
+  g_posted.erase(std::remove(g_posted.begin(), g_posted.end(), *request),
+                 g_posted.end());
+  g_reqs.erase(*request);
+  *request = MPI_REQUEST_NULL;
+  return MPI_SUCCESS;
+}
+
+int MPI_Get_count(const MPI_Status *status, MPI_Datatype datatype,
+                  int *count) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *t = get(datatype);
+  if (!t || !status)
+    return MPI_ERR_ARG;
+  if (t->size == 0) {
+    *count = 0;
+  } else if (status->bytes_ % t->size) {
+    *count = MPI_UNDEFINED;
+  } else {
+    *count = (int)(status->bytes_ / t->size);
+  }
+  return MPI_SUCCESS;
+}
+
+} // extern "C"

@@ -1,0 +1,277 @@
+// Batched pack/unpack: every region of a step in one launch.
+//
+// The reference packs one object per MPI_Pack call, each with its own launch
+// and stream synchronisation (src/pack.cpp:56, packer_2d.cu:101-109), so the
+// 26 halo regions of a 3-D grid cost 26 launches and 26 synchronisations.
+// Here the regions become a table in device memory; one grid-stride kernel
+// walks it.  The work is cut into equal chunks of kChunkWords words (one
+// chunk per CTA iteration); a region owns a contiguous range of chunks, found
+// by binary search over the table's prefix offsets.  Each region keeps its
+// own geometry and proven vector width, so a 16-B-row face and a 2-KiB-row
+// face run at their own best width inside the same launch.
+//
+// A batch can capture one launch into a CUDA graph and replay it; because
+// the pointers live in the table, replays see new buffer contents without
+// re-capture.
+
+#include "internal.hpp"
+
+#include <algorithm>
+#include <vector>
+
+namespace tempi {
+
+namespace {
+
+constexpr int kBatchThreads = 256;
+constexpr int kBatchUnroll = 4;
+constexpr uint32_t kChunkWords = kBatchThreads * kBatchUnroll;
+
+struct BatchRegion {
+  char *strided; // origin + start
+  char *packed;
+  Geometry g;
+  uint32_t chunk_begin; // first chunk of this region
+  uint32_t pad;
+};
+
+__device__ __forceinline__ uint32_t bdiv(uint32_t n, const FastDiv &f) {
+  return f.m ? (__umulhi(n, f.m) >> f.s) : n;
+}
+
+__device__ __forceinline__ int64_t brow_offset(uint32_t row, const Geometry &g) {
+  int64_t off = 0;
+#pragma unroll
+  for (int k = 0; k < KDIMS; ++k) {
+    if (k >= int(g.nd))
+      break;
+    if (k == int(g.nd) - 1) {
+      off += int64_t(row) * g.strides[k];
+    } else {
+      const uint32_t q = bdiv(row, g.cdiv[k]);
+      off += int64_t(row - q * g.cdiv[k].d) * g.strides[k];
+      row = q;
+    }
+  }
+  return off;
+}
+
+template <int W>
+__device__ __forceinline__ void copy_chunk(const BatchRegion &r, uint32_t w0,
+                                           bool unpack) {
+  using T = typename std::conditional<
+      W == 16, uint4,
+      typename std::conditional<
+          W == 8, uint2,
+          typename std::conditional<
+              W == 4, uint32_t,
+              typename std::conditional<W == 2, uint16_t,
+                                        uint8_t>::type>::type>::type>::type;
+  const Geometry &g = r.g;
+  const uint32_t total = g.total_words;
+  int64_t so[kBatchUnroll];
+  uint32_t ww[kBatchUnroll];
+#pragma unroll
+  for (int u = 0; u < kBatchUnroll; ++u) {
+    ww[u] = w0 + threadIdx.x + u * kBatchThreads;
+    if (ww[u] < total) {
+      const uint32_t row = bdiv(ww[u], g.wdiv);
+      so[u] = brow_offset(row, g) + int64_t(ww[u] - row * g.wpr) * W;
+    }
+  }
+  T v[kBatchUnroll];
+  if (!unpack) {
+#pragma unroll
+    for (int u = 0; u < kBatchUnroll; ++u)
+      if (ww[u] < total)
+        v[u] = __ldg(reinterpret_cast<const T *>(r.strided + so[u]));
+#pragma unroll
+    for (int u = 0; u < kBatchUnroll; ++u)
+      if (ww[u] < total)
+        reinterpret_cast<T *>(r.packed)[ww[u]] = v[u];
+  } else {
+#pragma unroll
+    for (int u = 0; u < kBatchUnroll; ++u)
+      if (ww[u] < total)
+        v[u] = __ldg(reinterpret_cast<const T *>(r.packed) + ww[u]);
+#pragma unroll
+    for (int u = 0; u < kBatchUnroll; ++u)
+      if (ww[u] < total)
+        *reinterpret_cast<T *>(r.strided + so[u]) = v[u];
+  }
+}
+
+__global__ void __launch_bounds__(kBatchThreads)
+    k_batch(const BatchRegion *__restrict__ regions, int nregions,
+            uint32_t total_chunks, int unpack) {
+  __shared__ BatchRegion sr;
+  __shared__ int cur;
+  if (threadIdx.x == 0)
+    cur = -1;
+  __syncthreads();
+  for (uint32_t chunk = blockIdx.x; chunk < total_chunks; chunk += gridDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = nregions - 1; // last region with chunk_begin <= chunk
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (regions[mid].chunk_begin <= chunk)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      if (lo != cur) {
+        sr = regions[lo];
+        cur = lo;
+      }
+    }
+    __syncthreads();
+    const uint32_t w0 = (chunk - sr.chunk_begin) * kChunkWords;
+    switch (sr.g.width) {
+    case 16: copy_chunk<16>(sr, w0, unpack); break;
+    case 8: copy_chunk<8>(sr, w0, unpack); break;
+    case 4: copy_chunk<4>(sr, w0, unpack); break;
+    case 2: copy_chunk<2>(sr, w0, unpack); break;
+    default: copy_chunk<1>(sr, w0, unpack); break;
+    }
+    __syncthreads();
+  }
+}
+
+} // namespace
+
+struct BatchImpl {
+  std::vector<BatchRegion> host;
+  BatchRegion *dev = nullptr;
+  uint32_t total_chunks = 0;
+  int unpack = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+} // namespace tempi
+
+struct tempi_batch {
+  tempi::BatchImpl impl;
+};
+
+using namespace tempi;
+
+extern "C" int tempi_batch_create(const tempi_region *regions, int32_t n,
+                                  int32_t unpack, tempi_batch **out) {
+  if (!out || n < 0 || (n > 0 && !regions))
+    return set_error(TEMPI_ERR_ARG, "bad batch arguments");
+  *out = nullptr;
+  auto *b = new tempi_batch();
+  b->impl.unpack = unpack ? 1 : 0;
+  uint64_t chunks = 0;
+  for (int32_t i = 0; i < n; ++i) {
+    const tempi_region &r = regions[i];
+    BatchRegion br{};
+    char *strided = (char *)r.origin + r.desc.start;
+    bool empty = false;
+    int err = make_geometry(&r.desc, r.incount, uintptr_t(strided),
+                            uintptr_t(r.packed), 0, &br.g, &empty);
+    if (err) {
+      delete b;
+      return err;
+    }
+    if (empty)
+      continue;
+    br.strided = strided;
+    br.packed = (char *)r.packed;
+    br.chunk_begin = uint32_t(chunks);
+    chunks += (br.g.total_words + kChunkWords - 1) / kChunkWords;
+    if (chunks > UINT32_MAX) {
+      delete b;
+      return set_error(TEMPI_ERR_ARG, "batch too large");
+    }
+    b->impl.host.push_back(br);
+  }
+  b->impl.total_chunks = uint32_t(chunks);
+  if (!b->impl.host.empty()) {
+    const size_t bytes = b->impl.host.size() * sizeof(BatchRegion);
+    cudaError_t e = cudaMalloc(&b->impl.dev, bytes);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(b->impl.dev, b->impl.host.data(), bytes,
+                     cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cudaFree(b->impl.dev);
+      delete b;
+      return cuda_error(e, "batch table upload");
+    }
+  }
+  *out = b;
+  return TEMPI_OK;
+}
+
+static int batch_launch(tempi_batch *b, cudaStream_t s) {
+  BatchImpl &bi = b->impl;
+  if (bi.host.empty())
+    return TEMPI_OK;
+  const int sms = num_sms();
+  const uint32_t grid =
+      std::max<uint32_t>(1, std::min<uint32_t>(bi.total_chunks, sms * 8));
+  k_batch<<<grid, kBatchThreads, 0, s>>>(bi.dev, int(bi.host.size()),
+                                        bi.total_chunks, bi.unpack);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return cuda_error(e, "batch launch");
+  counters().kernel_launches++;
+  set_last_kernel(bi.unpack ? "batch_unpack" : "batch_pack");
+  return TEMPI_OK;
+}
+
+extern "C" int tempi_batch_launch(tempi_batch *b, void *stream) {
+  if (!b)
+    return set_error(TEMPI_ERR_ARG, "null batch");
+  return batch_launch(b, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int tempi_batch_capture(tempi_batch *b, void *stream) {
+  if (!b)
+    return set_error(TEMPI_ERR_ARG, "null batch");
+  BatchImpl &bi = b->impl;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (bi.exec) {
+    cudaGraphExecDestroy(bi.exec);
+    cudaGraphDestroy(bi.graph);
+    bi.exec = nullptr;
+    bi.graph = nullptr;
+  }
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess)
+    return cuda_error(e, "begin capture");
+  int err = batch_launch(b, s);
+  e = cudaStreamEndCapture(s, &bi.graph);
+  if (err)
+    return err;
+  if (e != cudaSuccess)
+    return cuda_error(e, "end capture");
+  e = cudaGraphInstantiate(&bi.exec, bi.graph, 0);
+  if (e != cudaSuccess)
+    return cuda_error(e, "graph instantiate");
+  return TEMPI_OK;
+}
+
+extern "C" int tempi_batch_replay(tempi_batch *b, void *stream) {
+  if (!b || !b->impl.exec)
+    return set_error(TEMPI_ERR_ARG, "batch has no captured graph");
+  cudaError_t e = cudaGraphLaunch(b->impl.exec, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess)
+    return cuda_error(e, "graph launch");
+  if (!b->impl.host.empty())
+    counters().kernel_launches++;
+  return TEMPI_OK;
+}
+
+extern "C" int tempi_batch_destroy(tempi_batch *b) {
+  if (!b)
+    return TEMPI_OK;
+  if (b->impl.exec)
+    cudaGraphExecDestroy(b->impl.exec);
+  if (b->impl.graph)
+    cudaGraphDestroy(b->impl.graph);
+  cudaFree(b->impl.dev);
+  delete b;
+  return TEMPI_OK;
+}

@@ -1,0 +1,109 @@
+// Internal declarations shared by the host and device sources of
+// libtempi_b200.so.  Nothing here is part of the public ABI.
+#pragma once
+
+#include "tempi_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+
+namespace tempi {
+
+// ---- logging ------------------------------------------------------------
+// TEMPI_LOG_LEVEL: 0 silent (default), 1 errors, 2 warnings, 3 info, 4 debug
+int log_level();
+#define TEMPI_LOG(lvl, tag, ...)                                               \
+  do {                                                                         \
+    if (::tempi::log_level() >= (lvl)) {                                       \
+      std::fprintf(stderr, "[tempi " tag "] " __VA_ARGS__);                    \
+      std::fputc('\n', stderr);                                                \
+    }                                                                          \
+  } while (0)
+#define LOG_ERROR(...) TEMPI_LOG(1, "error", __VA_ARGS__)
+#define LOG_WARN(...) TEMPI_LOG(2, "warn", __VA_ARGS__)
+#define LOG_INFO(...) TEMPI_LOG(3, "info", __VA_ARGS__)
+#define LOG_DEBUG(...) TEMPI_LOG(4, "debug", __VA_ARGS__)
+
+// record a message for tempi_last_error() and return `code`
+int set_error(int code, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what);
+
+// ---- counters (reference include/counters.hpp:14-115) ----------------------
+struct Counters {
+  std::atomic<int64_t> kernel_launches{0};
+  std::atomic<int64_t> packs{0}, unpacks{0};
+  std::atomic<int64_t> pack_bytes{0}, unpack_bytes{0};
+  std::atomic<int64_t> lib_pack{0}, lib_unpack{0};
+  std::atomic<int64_t> send_device{0}, send_oneshot{0}, send_staged{0},
+      send_lib{0};
+  std::atomic<int64_t> recv_device{0}, recv_oneshot{0}, recv_staged{0},
+      recv_lib{0};
+  std::atomic<int64_t> isend_managed{0}, irecv_managed{0};
+  std::atomic<int64_t> dispatch_hit{0}, dispatch_miss{0};
+  std::atomic<int64_t> slab_hits{0}, slab_misses{0}, slab_bytes{0};
+  std::atomic<int64_t> cached_types{0};
+};
+Counters &counters();
+
+// last kernel variant name, for tests and profiling
+void set_last_kernel(const char *name);
+
+// ---- launch geometry ------------------------------------------------------
+
+constexpr int KDIMS = TEMPI_MAX_DIMS + 1; // strided dims plus the object count
+
+// Exact division of n < 2^31 by an invariant d < 2^31 with one multiply-high
+// and a shift: the round-up method of Granlund and Montgomery, "Division by
+// invariant integers using multiplication" (PLDI 1994).  With
+// l = ceil(log2 d) and m = ceil(2^(31+l) / d) < 2^32, floor(n/d) =
+// floor(n*m / 2^(31+l)) for all n < 2^31, i.e. umulhi(n, m) >> (l-1).
+struct FastDiv {
+  uint32_t d, m, s;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f{d, 0, 0};
+  if (d <= 1)
+    return f;
+  uint32_t l = 32 - __builtin_clz(d - 1);
+  uint64_t m = ((uint64_t(1) << (31 + l)) + d - 1) / d;
+  f.m = (uint32_t)m;
+  f.s = l - 1;
+  return f;
+}
+
+// A normalised launch: rows of `block` bytes; row r splits into digits over
+// counts (fastest first); the strided side of row r starts at
+// base + sum digit_k * strides[k]; the packed side at packed + r*block.
+struct Geometry {
+  int64_t strides[KDIMS];
+  FastDiv cdiv[KDIMS];
+  uint32_t nd;    // strided dims in use (0..KDIMS)
+  uint32_t width; // bytes per vector word
+  uint32_t wpr;   // words per row
+  FastDiv wdiv;   // divides by wpr
+  uint32_t rows;
+  uint32_t total_words; // rows * wpr, < 2^31
+  int64_t block;
+};
+
+// Build a normalised geometry for `incount` objects of `d` with the given
+// base pointers.  Folds unit dims, merges dims that are contiguous with each
+// other and proves the widest vector width.  Returns TEMPI_OK, or an error;
+// sets *empty when there is nothing to copy.
+int make_geometry(const tempi_desc *d, int64_t incount, uintptr_t strided_base,
+                  uintptr_t packed_base, int max_width, Geometry *g,
+                  bool *empty);
+
+// Launch one pack (unpack=false) or unpack on `stream`.
+int launch_geometry(const Geometry &g, const char *strided_base, char *packed,
+                    bool unpack, const tempi_config *cfg, cudaStream_t stream);
+
+int num_sms();
+
+} // namespace tempi

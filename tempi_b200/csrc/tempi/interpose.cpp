@@ -1,0 +1,269 @@
+// The interposed MPI entry points.  Each follows the reference's decision
+// order (src/pack.cpp, src/unpack.cpp, src/type_commit.cpp,
+// src/type_free.cpp, src/internal/send.cpp, src/recv.cpp,
+// src/internal/isend.cpp, src/internal/irecv.cpp, src/wait.cpp) with these
+// changes:
+//  * errors come back as MPI error codes; nothing calls exit();
+//  * MPI_Pack/MPI_Unpack check outsize/insize (MPI_ERR_TRUNCATE, nothing
+//    written), which the reference does not;
+//  * a committed type that TEMPI cannot describe goes to the library instead
+//    of dereferencing a null packer;
+//  * once TEMPI has taken a call onto the GPU path it never falls back to a
+//    CPU copy: a CUDA failure is returned as MPI_ERR_OTHER.
+
+#include "dispatch.hpp"
+#include "runtime.hpp"
+#include "sender.hpp"
+
+namespace tempi {
+namespace {
+
+bool ready() { return resolve_symbols(); }
+
+int to_mpi(int e) {
+  switch (e) {
+  case TEMPI_OK: return MPI_SUCCESS;
+  case TEMPI_ERR_TRUNCATE: return MPI_ERR_TRUNCATE;
+  case TEMPI_ERR_ARG: return MPI_ERR_ARG;
+  case TEMPI_ERR_NO_MEM: return MPI_ERR_NO_MEM;
+  default: return MPI_ERR_OTHER;
+  }
+}
+
+void on_init() {
+  read_env();
+  dispatch_init();
+}
+
+void on_finalize() {
+  async_finalize();
+  slab_release_all();
+  events_release_all();
+}
+
+} // namespace
+} // namespace tempi
+
+using namespace tempi;
+
+extern "C" {
+
+int MPI_Init(int *argc, char ***argv) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  int err = libmpi.Init(argc, argv);
+  if (err == MPI_SUCCESS)
+    on_init();
+  return err;
+}
+
+int MPI_Init_thread(int *argc, char ***argv, int required, int *provided) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  int err = libmpi.Init_thread(argc, argv, required, provided);
+  if (err == MPI_SUCCESS)
+    on_init();
+  return err;
+}
+
+int MPI_Finalize(void) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  if (!env().disable)
+    on_finalize();
+  return libmpi.Finalize();
+}
+
+int MPI_Type_commit(MPI_Datatype *datatype) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  int err = libmpi.Type_commit(datatype);
+  if (err != MPI_SUCCESS || env().disable || env().no_type_commit)
+    return err;
+  commit_type(*datatype);
+  return err;
+}
+
+int MPI_Type_free(MPI_Datatype *datatype) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  if (!env().disable && !env().no_type_commit && datatype)
+    release_type(*datatype); // before the library may reuse the handle
+  return libmpi.Type_free(datatype);
+}
+
+int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
+             void *outbuf, int outsize, int *position, MPI_Comm comm) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  if (env().disable || env().no_pack)
+    return libmpi.Pack(inbuf, incount, datatype, outbuf, outsize, position,
+                       comm);
+  TypeRecord *r = find_type(datatype);
+  if (!r || !r->packable) {
+    counters().lib_pack++;
+    return libmpi.Pack(inbuf, incount, datatype, outbuf, outsize, position,
+                       comm);
+  }
+  PtrInfo in = classify(inbuf), out = classify(outbuf);
+  if (!in.device_accessible || !out.device_accessible) {
+    counters().lib_pack++;
+    return libmpi.Pack(inbuf, incount, datatype, outbuf, outsize, position,
+                       comm);
+  }
+  if (!position || incount < 0)
+    return MPI_ERR_ARG;
+  const int64_t bytes = int64_t(incount) * r->desc.size;
+  if (*position < 0 || *position + bytes > int64_t(outsize))
+    return MPI_ERR_TRUNCATE;
+  cudaStream_t s = pack_stream();
+  tempi_config cfg = choose_config(r->desc, incount);
+  int e = tempi_pack(&r->desc, in.device_ptr, incount,
+                     static_cast<char *>(out.device_ptr) + *position, &cfg, s);
+  if (!e) {
+    cudaError_t ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess)
+      e = cuda_error(ce, "MPI_Pack synchronize");
+  }
+  if (e)
+    return to_mpi(e);
+  *position += int(bytes);
+  return MPI_SUCCESS;
+}
+
+int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
+               int outcount, MPI_Datatype datatype, MPI_Comm comm) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  if (env().disable || env().no_pack)
+    return libmpi.Unpack(inbuf, insize, position, outbuf, outcount, datatype,
+                         comm);
+  TypeRecord *r = find_type(datatype);
+  if (!r || !r->packable) {
+    counters().lib_unpack++;
+    return libmpi.Unpack(inbuf, insize, position, outbuf, outcount, datatype,
+                         comm);
+  }
+  PtrInfo in = classify(inbuf), out = classify(outbuf);
+  if (!in.device_accessible || !out.device_accessible) {
+    counters().lib_unpack++;
+    return libmpi.Unpack(inbuf, insize, position, outbuf, outcount, datatype,
+                         comm);
+  }
+  if (!position || outcount < 0)
+    return MPI_ERR_ARG;
+  const int64_t bytes = int64_t(outcount) * r->desc.size;
+  if (*position < 0 || *position + bytes > int64_t(insize))
+    return MPI_ERR_TRUNCATE;
+  cudaStream_t s = pack_stream();
+  tempi_config cfg = choose_config(r->desc, outcount);
+  int e = tempi_unpack(&r->desc,
+                       static_cast<const char *>(in.device_ptr) + *position,
+                       outcount, out.device_ptr, &cfg, s);
+  if (!e) {
+    cudaError_t ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess)
+      e = cuda_error(ce, "MPI_Unpack synchronize");
+  }
+  if (e)
+    return to_mpi(e);
+  *position += int(bytes);
+  return MPI_SUCCESS;
+}
+
+int MPI_Send(const void *buf, int count, MPI_Datatype datatype, int dest,
+             int tag, MPI_Comm comm) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  if (env().disable)
+    return libmpi.Send(buf, count, datatype, dest, tag, comm);
+  PtrInfo p = classify(buf);
+  TypeRecord *r = p.device_accessible ? find_type(datatype) : nullptr;
+  if (r && r->packable && r->desc.ndims >= 1 && count > 0) {
+    Method m = choose_method(*r, count);
+    return send_strided(*r, m, p.device_ptr, count, dest, tag, comm);
+  }
+  if (r && r->packable && r->desc.ndims == 0 && count > 0 &&
+      env().contiguous == Contiguous::STAGED && p.is_device) {
+    return send_contiguous_staged(buf, count, datatype,
+                                  int64_t(count) * r->desc.size, dest, tag,
+                                  comm);
+  }
+  counters().send_lib++;
+  return libmpi.Send(buf, count, datatype, dest, tag, comm);
+}
+
+int MPI_Recv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
+             MPI_Comm comm, MPI_Status *status) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  if (env().disable)
+    return libmpi.Recv(buf, count, datatype, source, tag, comm, status);
+  PtrInfo p = classify(buf);
+  TypeRecord *r = p.device_accessible ? find_type(datatype) : nullptr;
+  if (r && r->packable && r->desc.ndims >= 1 && count > 0) {
+    Method m = choose_method(*r, count);
+    return recv_strided(*r, m, p.device_ptr, count, source, tag, comm, status);
+  }
+  if (r && r->packable && r->desc.ndims == 0 && count > 0 &&
+      env().contiguous == Contiguous::STAGED && p.is_device) {
+    return recv_contiguous_staged(buf, count, datatype,
+                                  int64_t(count) * r->desc.size, source, tag,
+                                  comm, status);
+  }
+  counters().recv_lib++;
+  return libmpi.Recv(buf, count, datatype, source, tag, comm, status);
+}
+
+int MPI_Isend(const void *buf, int count, MPI_Datatype datatype, int dest,
+              int tag, MPI_Comm comm, MPI_Request *request) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  if (env().disable)
+    return libmpi.Isend(buf, count, datatype, dest, tag, comm, request);
+  PtrInfo p = classify(buf);
+  TypeRecord *r = p.device_accessible ? find_type(datatype) : nullptr;
+  int err;
+  if (r && r->packable && r->desc.ndims >= 1 && count > 0) {
+    Method m = choose_method(*r, count);
+    err = start_isend(*r, m, p.device_ptr, count, dest, tag, comm, request);
+  } else {
+    err = libmpi.Isend(buf, count, datatype, dest, tag, comm, request);
+  }
+  try_progress();
+  return err;
+}
+
+int MPI_Irecv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
+              MPI_Comm comm, MPI_Request *request) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  if (env().disable)
+    return libmpi.Irecv(buf, count, datatype, source, tag, comm, request);
+  PtrInfo p = classify(buf);
+  TypeRecord *r = p.device_accessible ? find_type(datatype) : nullptr;
+  int err;
+  if (r && r->packable && r->desc.ndims >= 1 && count > 0) {
+    Method m = choose_method(*r, count);
+    err = start_irecv(*r, m, p.device_ptr, count, source, tag, comm, request);
+  } else {
+    err = libmpi.Irecv(buf, count, datatype, source, tag, comm, request);
+  }
+  try_progress();
+  return err;
+}
+
+int MPI_Wait(MPI_Request *request, MPI_Status *status) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  if (env().disable || !request || !is_managed(*request)) {
+    // an unmanaged receive may match a managed send whose pack is in flight
+    int e = progress_sends();
+    if (e)
+      return e;
+    return libmpi.Wait(request, status);
+  }
+  return wait_managed(request, status);
+}
+
+} // extern "C"

@@ -1,0 +1,372 @@
+// Strided pack / unpack kernels for sm_100a.
+//
+// What they compute is the reference packers' job (pack_2d/unpack_2d,
+// include/pack_kernels.cuh:64-120; pack_3d/unpack_3d, :350-433; Packer1D's
+// cudaMemcpyAsync, src/internal/packer_1d.cu:16-50): copy the described bytes
+// of `incount` objects, in type-map order, to or from a contiguous buffer.
+//
+// How is this library's own design:
+//  * one launch covers every object: the object count is just the slowest
+//    strided dimension (stride = extent), and dimensions that are contiguous
+//    with each other are merged on the host first (make_geometry);
+//  * offsets are 64-bit; rows and words are 32-bit indices (packed sizes are
+//    bounded by MPI's int counts), decomposed with exact multiply-high
+//    division (FastDiv) instead of hardware division;
+//  * the vector width is the widest power of two (up to 16 B) that divides
+//    the block length, every stride and BOTH runtime base pointers, so every
+//    access is naturally aligned (the reference checks only block length and
+//    start offset, pack_kernels.cuh:129-157, and never uses 16-B words);
+//  * k_words: one thread per output word, U independent loads in flight per
+//    thread; packed-side accesses are contiguous across a warp.  Used for
+//    short rows, where a warp spans many rows.
+//  * k_rows: one warp per row, lanes stride across the row's words, U loads
+//    in flight per lane; the row offset is computed once per row.  Used for
+//    wide rows.
+//  * grids are a multiple of the SM count and grid-stride over the work.
+
+#include "internal.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+namespace tempi {
+
+template <int W> struct Word;
+template <> struct Word<1> { using T = uint8_t; };
+template <> struct Word<2> { using T = uint16_t; };
+template <> struct Word<4> { using T = uint32_t; };
+template <> struct Word<8> { using T = uint2; };
+template <> struct Word<16> { using T = uint4; };
+
+__device__ __forceinline__ uint32_t fastdiv(uint32_t n, const FastDiv &f) {
+  return f.m ? (__umulhi(n, f.m) >> f.s) : n;
+}
+
+template <int ND>
+__device__ __forceinline__ int64_t row_offset(uint32_t row, const Geometry &g) {
+  int64_t off = 0;
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    if (k == ND - 1) {
+      off += int64_t(row) * g.strides[k];
+    } else {
+      const uint32_t q = fastdiv(row, g.cdiv[k]);
+      off += int64_t(row - q * g.cdiv[k].d) * g.strides[k];
+      row = q;
+    }
+  }
+  return off;
+}
+
+constexpr int kUnroll = 4;
+
+template <int W, int ND, bool UNPACK>
+__global__ void __launch_bounds__(512)
+    k_words(char *__restrict__ strided, char *__restrict__ packed,
+            const __grid_constant__ Geometry g) {
+  using T = typename Word<W>::T;
+  constexpr int U = kUnroll;
+  const uint32_t nthreads = gridDim.x * blockDim.x;
+  const uint32_t total = g.total_words;
+  uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+
+  for (; w + (U - 1) * nthreads < total; w += U * nthreads) {
+    int64_t so[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint32_t ww = w + u * nthreads;
+      const uint32_t row = fastdiv(ww, g.wdiv);
+      const uint32_t col = ww - row * g.wpr;
+      so[u] = row_offset<ND>(row, g) + int64_t(col) * W;
+    }
+    T v[U];
+    if (!UNPACK) {
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        v[u] = __ldg(reinterpret_cast<const T *>(strided + so[u]));
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        reinterpret_cast<T *>(packed)[w + u * nthreads] = v[u];
+    } else {
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        v[u] = __ldg(reinterpret_cast<const T *>(packed) + (w + u * nthreads));
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        *reinterpret_cast<T *>(strided + so[u]) = v[u];
+    }
+  }
+  for (; w < total; w += nthreads) {
+    const uint32_t row = fastdiv(w, g.wdiv);
+    const uint32_t col = w - row * g.wpr;
+    const int64_t so = row_offset<ND>(row, g) + int64_t(col) * W;
+    if (!UNPACK)
+      reinterpret_cast<T *>(packed)[w] =
+          __ldg(reinterpret_cast<const T *>(strided + so));
+    else
+      *reinterpret_cast<T *>(strided + so) =
+          __ldg(reinterpret_cast<const T *>(packed) + w);
+  }
+}
+
+template <int W, int ND, bool UNPACK>
+__global__ void __launch_bounds__(512)
+    k_rows(char *__restrict__ strided, char *__restrict__ packed,
+           const __grid_constant__ Geometry g) {
+  using T = typename Word<W>::T;
+  constexpr int U = kUnroll;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t wpr = g.wpr;
+  for (uint32_t row = warp; row < g.rows; row += nwarps) {
+    T *s = reinterpret_cast<T *>(strided + row_offset<ND>(row, g));
+    T *p = reinterpret_cast<T *>(packed + int64_t(row) * g.block);
+    const T *src = UNPACK ? p : s;
+    T *dst = UNPACK ? s : p;
+    uint32_t c = lane;
+    for (; c + 32 * (U - 1) < wpr; c += 32 * U) {
+      T v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        v[u] = __ldg(src + c + 32 * u);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        dst[c + 32 * u] = v[u];
+    }
+    for (; c < wpr; c += 32)
+      dst[c] = __ldg(src + c);
+  }
+}
+
+using KernelFn = void (*)(char *, char *, Geometry);
+
+template <int W, bool UNPACK> KernelFn pick_words(uint32_t nd) {
+  switch (nd) {
+  case 0: return k_words<W, 0, UNPACK>;
+  case 1: return k_words<W, 1, UNPACK>;
+  case 2: return k_words<W, 2, UNPACK>;
+  case 3: return k_words<W, 3, UNPACK>;
+  case 4: return k_words<W, 4, UNPACK>;
+  default: return k_words<W, 5, UNPACK>;
+  }
+}
+
+template <int W, bool UNPACK> KernelFn pick_rows(uint32_t nd) {
+  switch (nd) {
+  case 0: return k_rows<W, 0, UNPACK>;
+  case 1: return k_rows<W, 1, UNPACK>;
+  case 2: return k_rows<W, 2, UNPACK>;
+  case 3: return k_rows<W, 3, UNPACK>;
+  case 4: return k_rows<W, 4, UNPACK>;
+  default: return k_rows<W, 5, UNPACK>;
+  }
+}
+
+template <bool UNPACK> KernelFn pick(int kernel, uint32_t width, uint32_t nd) {
+  if (kernel == 2) {
+    switch (width) {
+    case 16: return pick_rows<16, UNPACK>(nd);
+    case 8: return pick_rows<8, UNPACK>(nd);
+    case 4: return pick_rows<4, UNPACK>(nd);
+    case 2: return pick_rows<2, UNPACK>(nd);
+    default: return pick_rows<1, UNPACK>(nd);
+    }
+  }
+  switch (width) {
+  case 16: return pick_words<16, UNPACK>(nd);
+  case 8: return pick_words<8, UNPACK>(nd);
+  case 4: return pick_words<4, UNPACK>(nd);
+  case 2: return pick_words<2, UNPACK>(nd);
+  default: return pick_words<1, UNPACK>(nd);
+  }
+}
+
+static const char *kernel_name(int kernel, uint32_t width, bool unpack) {
+  static char names[2][2][17][32];
+  static std::once_flag once;
+  std::call_once(once, [] {
+    for (int k = 0; k < 2; ++k)
+      for (int u = 0; u < 2; ++u)
+        for (int w = 1; w <= 16; w *= 2)
+          std::snprintf(names[k][u][w], 32, "%s_%s_w%d",
+                        k ? "rows" : "words", u ? "unpack" : "pack", w);
+  });
+  return names[kernel == 2][unpack][width];
+}
+
+int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+            cudaSuccess) {
+      cudaGetLastError();
+      sms = 148;
+    }
+  }
+  return sms;
+}
+
+int make_geometry(const tempi_desc *d, int64_t incount, uintptr_t sbase,
+                  uintptr_t pbase, int max_width, Geometry *g, bool *empty) {
+  *empty = false;
+  if (!d || !g)
+    return set_error(TEMPI_ERR_ARG, "null descriptor");
+  if (d->ndims < 0 || d->ndims > TEMPI_MAX_DIMS || d->block < 0 || incount < 0)
+    return set_error(TEMPI_ERR_ARG, "bad descriptor (ndims=%d block=%lld)",
+                     d->ndims, (long long)d->block);
+  if (incount == 0 || d->block == 0) {
+    *empty = true;
+    return TEMPI_OK;
+  }
+  int64_t cnt[KDIMS], str[KDIMS];
+  int n = 0;
+  for (int k = 0; k < d->ndims; ++k) {
+    if (d->counts[k] < 0)
+      return set_error(TEMPI_ERR_ARG, "negative count");
+    if (d->counts[k] == 0) {
+      *empty = true;
+      return TEMPI_OK;
+    }
+    if (d->counts[k] != 1) {
+      cnt[n] = d->counts[k];
+      str[n] = d->strides[k];
+      ++n;
+    }
+  }
+  if (incount != 1) {
+    cnt[n] = incount;
+    str[n] = d->extent;
+    ++n;
+  }
+  int64_t block = d->block;
+  for (bool changed = true; changed;) {
+    changed = false;
+    if (n > 0 && str[0] == block) { // rows are adjacent: one longer block
+      block *= cnt[0];
+      for (int k = 1; k < n; ++k)
+        cnt[k - 1] = cnt[k], str[k - 1] = str[k];
+      --n;
+      changed = true;
+      continue;
+    }
+    for (int k = 0; k + 1 < n; ++k) {
+      if (str[k + 1] == cnt[k] * str[k]) { // dim k+1 continues dim k
+        cnt[k] *= cnt[k + 1];
+        for (int j = k + 2; j < n; ++j)
+          cnt[j - 1] = cnt[j], str[j - 1] = str[j];
+        --n;
+        changed = true;
+        break;
+      }
+    }
+  }
+  int64_t rows = 1;
+  for (int k = 0; k < n; ++k) {
+    rows *= cnt[k];
+    if (rows > INT32_MAX)
+      return set_error(TEMPI_ERR_ARG, "too many rows");
+  }
+  if (block > INT32_MAX || rows * block > INT32_MAX)
+    return set_error(TEMPI_ERR_ARG, "packed size exceeds 2^31-1 bytes");
+  for (int k = 0; k < n; ++k)
+    if (cnt[k] > INT32_MAX)
+      return set_error(TEMPI_ERR_ARG, "count too large");
+
+  uint64_t bits = uint64_t(block) | uint64_t(sbase) | uint64_t(pbase);
+  for (int k = 0; k < n; ++k)
+    bits |= uint64_t(str[k]);
+  uint32_t w = 16;
+  while (w > 1 && (bits & (w - 1)))
+    w >>= 1;
+  while (max_width > 0 && w > uint32_t(max_width))
+    w >>= 1;
+
+  std::memset(g, 0, sizeof(*g));
+  g->nd = n;
+  for (int k = 0; k < n; ++k) {
+    g->strides[k] = str[k];
+    g->cdiv[k] = make_fastdiv(uint32_t(cnt[k]));
+  }
+  g->width = w;
+  g->wpr = uint32_t(block / w);
+  g->wdiv = make_fastdiv(g->wpr);
+  g->rows = uint32_t(rows);
+  g->total_words = uint32_t(rows) * g->wpr;
+  g->block = block;
+  return TEMPI_OK;
+}
+
+int launch_geometry(const Geometry &g, const char *strided, char *packed,
+                    bool unpack, const tempi_config *cfg,
+                    cudaStream_t stream) {
+  const int sms = num_sms();
+  int kernel = cfg ? cfg->kernel : 0;
+  if (kernel != 1 && kernel != 2)
+    kernel = (g.wpr >= 64 && g.rows >= uint32_t(2 * sms)) ? 2 : 1;
+  int threads = (cfg && cfg->threads) ? cfg->threads : 256;
+  threads = std::max(32, std::min(512, threads / 32 * 32));
+  int bps = (cfg && cfg->blocks_per_sm) ? cfg->blocks_per_sm : 2048 / threads;
+  int64_t need;
+  if (kernel == 2)
+    need = (int64_t(g.rows) * 32 + threads - 1) / threads;
+  else
+    need = (int64_t(g.total_words) + int64_t(threads) * kUnroll - 1) /
+           (int64_t(threads) * kUnroll);
+  int64_t blocks = std::min<int64_t>(need, int64_t(sms) * bps);
+  blocks = std::max<int64_t>(blocks, 1);
+  KernelFn fn = unpack ? pick<true>(kernel, g.width, g.nd)
+                       : pick<false>(kernel, g.width, g.nd);
+  fn<<<unsigned(blocks), threads, 0, stream>>>(const_cast<char *>(strided),
+                                               packed, g);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return cuda_error(e, "pack kernel launch");
+  counters().kernel_launches++;
+  set_last_kernel(kernel_name(kernel, g.width, unpack));
+  return TEMPI_OK;
+}
+
+} // namespace tempi
+
+using namespace tempi;
+
+extern "C" int tempi_pack(const tempi_desc *d, const void *origin,
+                          int64_t incount, void *packed,
+                          const tempi_config *cfg, void *stream) {
+  if (!d)
+    return set_error(TEMPI_ERR_ARG, "null descriptor");
+  const char *base = static_cast<const char *>(origin) + d->start;
+  Geometry g;
+  bool empty;
+  int err = make_geometry(d, incount, uintptr_t(base), uintptr_t(packed),
+                          cfg ? cfg->width : 0, &g, &empty);
+  if (err || empty)
+    return err;
+  counters().packs++;
+  counters().pack_bytes += int64_t(g.rows) * g.block;
+  return launch_geometry(g, base, static_cast<char *>(packed), false, cfg,
+                         static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int tempi_unpack(const tempi_desc *d, const void *packed,
+                            int64_t incount, void *origin,
+                            const tempi_config *cfg, void *stream) {
+  if (!d)
+    return set_error(TEMPI_ERR_ARG, "null descriptor");
+  char *base = static_cast<char *>(origin) + d->start;
+  Geometry g;
+  bool empty;
+  int err = make_geometry(d, incount, uintptr_t(base), uintptr_t(packed),
+                          cfg ? cfg->width : 0, &g, &empty);
+  if (err || empty)
+    return err;
+  counters().unpacks++;
+  counters().unpack_bytes += int64_t(g.rows) * g.block;
+  return launch_geometry(g, base, const_cast<char *>(
+                                      static_cast<const char *>(packed)),
+                         true, cfg, static_cast<cudaStream_t>(stream));
+}

@@ -1,0 +1,80 @@
+// Host runtime of the interposer: environment knobs, type cache, device
+// stream, slab allocators and event pool.
+#pragma once
+
+#include "internal.hpp"
+#include "symbols.hpp"
+
+#include <cstddef>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+namespace tempi {
+
+// ---- environment (reference include/env.hpp:10-37, src/internal/env.cpp) --
+enum class Method { AUTO = 0, DEVICE = 1, ONESHOT = 2, STAGED = 3 };
+enum class Contiguous { NONE, AUTO, STAGED };
+enum class Dispatch { LEARNED, TABLE, EXHAUSTIVE, HEURISTIC };
+
+struct Env {
+  bool disable = false;      // TEMPI_DISABLE
+  bool no_pack = false;      // TEMPI_NO_PACK
+  bool no_type_commit = false; // TEMPI_NO_TYPE_COMMIT
+  Method datatype = Method::AUTO; // TEMPI_DATATYPE_{ONESHOT,DEVICE,STAGED,AUTO}
+  Contiguous contiguous = Contiguous::NONE; // TEMPI_CONTIGUOUS_{STAGED,AUTO}
+  Dispatch dispatch = Dispatch::LEARNED; // TEMPI_DISPATCH=learned|table|exhaustive|heuristic
+  std::string cache_dir;     // TEMPI_CACHE_DIR
+  double wait_timeout_s = 30; // TEMPI_WAIT_TIMEOUT_S: bound on MPI_Wait polling
+};
+const Env &env();
+void read_env(); // re-read the environment (MPI_Init does this)
+
+// ---- canonicaliser ---------------------------------------------------------
+// Describe `t` as a strided block; TEMPI_ERR_UNSUPPORTED when it is not one.
+int canonicalize(MPI_Datatype t, tempi_desc *out);
+
+// ---- type cache (reference include/type_cache.hpp:23-30) ------------------
+struct TypeRecord {
+  tempi_desc desc{};
+  bool packable = false; // desc describes the type and a kernel handles it
+  // method chosen per packed byte count (reference SendRecvND's
+  // modelChoiceCache_, sender.cpp:259-277)
+  std::unordered_map<int64_t, Method> methods;
+};
+
+// Returns nullptr when the type is unknown.  The pointer stays valid until
+// the type is released.
+TypeRecord *find_type(MPI_Datatype t);
+TypeRecord *commit_type(MPI_Datatype t);
+void release_type(MPI_Datatype t);
+
+// ---- device state ---------------------------------------------------------
+// Lazily creates TEMPI's non-blocking stream on the current device
+// (reference kernStream, src/internal/streams.cpp:19-28).
+cudaStream_t pack_stream();
+bool cuda_available();
+
+// Where a pointer lives.  device_ptr is what a kernel should use.
+struct PtrInfo {
+  bool device_accessible = false; // device memory, managed, or mapped host
+  bool is_device = false;         // device memory proper
+  void *device_ptr = nullptr;
+};
+PtrInfo classify(const void *p);
+
+// ---- slab allocators (reference include/allocator_slab.hpp) ---------------
+// Power-of-two size classes with O(1) free lists.  Device slabs come from
+// cudaMalloc; host slabs from cudaHostAlloc(Mapped|Portable), so kernels can
+// write them directly (the ONE_SHOT path).
+enum class Space { DEVICE, HOST_MAPPED };
+void *slab_alloc(Space s, size_t bytes);
+void slab_free(Space s, void *p);
+void slab_release_all();
+
+// ---- event pool (reference src/internal/events.cpp:17-86) -----------------
+cudaEvent_t event_acquire();
+void event_release(cudaEvent_t e);
+void events_release_all();
+
+} // namespace tempi

@@ -1,0 +1,136 @@
+"""Batched halo pack/unpack (benchmark config 3 at test sizes): one launch,
+or one CUDA-graph replay, must write exactly what 26 per-region MPI_Pack
+calls write, and the unpack must fill exactly the ghost cells."""
+import numpy as np
+import pytest
+
+from oracle import types as T
+from tempi_b200 import _lib, halo, mpi
+
+from . import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_grid_types(g: halo.Grid, ghost: bool):
+    out = {}
+    sizes = [g.alloc[2], g.alloc[1], g.alloc[0]]
+    for d in halo.directions():
+        subs, starts = g.region_shape[(d, ghost)]
+        out[d] = T.subarray(sizes, subs, starts, T.ORDER_C, T.named(g.elem_bytes))
+    return out
+
+
+def oracle_pack(g, data):
+    ts = oracle_grid_types(g, False)
+    return np.concatenate([T.pack(ts[d], data, 1) for d in halo.directions()])
+
+
+def oracle_unpack(g, packed, data):
+    ts = oracle_grid_types(g, True)
+    offs = g.offsets()
+    out = data.copy()
+    for d in halo.directions():
+        t = ts[tuple(-x for x in d)]
+        T.unpack(t, packed[offs[d]: offs[d] + t.size], out, 1)
+    return out
+
+
+def test_halo_26_regions_sizes(mpi_init):
+    g = halo.Grid((256, 256, 256), 2)
+    # 6 faces 256*256*2, 12 edges 256*2*2, 8 corners 2*2*2 doubles
+    assert g.packed_bytes == 8 * (6 * 256 * 256 * 2 + 12 * 256 * 4 + 8 * 8) == 6390272
+
+
+@pytest.mark.parametrize("interior,radius", [((20, 17, 9), 2), ((33, 8, 12), 1), ((16, 16, 16), 3)])
+def test_batch_matches_plain_and_oracle(cuda, mpi_init, interior, radius):
+    import torch
+
+    g = halo.Grid(interior, radius)
+    data_np = H.splitmix_bytes(g.nbytes, radius)
+    data = torch.from_numpy(data_np).cuda()
+    p_batch = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
+    p_plain = torch.zeros_like(p_batch)
+    torch.cuda.synchronize()
+    assert halo.pack_plain(g, data.data_ptr(), p_plain.data_ptr()) == g.packed_bytes
+    b = halo.HaloBatch([g], [data.data_ptr()], [p_batch.data_ptr()])
+    assert b.nregions == 26
+    b.launch()
+    torch.cuda.synchronize()
+    want = oracle_pack(g, data_np)
+    assert p_plain.cpu().numpy().tobytes() == want.tobytes()
+    assert p_batch.cpu().numpy().tobytes() == want.tobytes()
+
+    # unpack into ghost cells, batched and plain
+    ghost = torch.from_numpy(data_np.copy()).cuda()
+    ghost2 = ghost.clone()
+    ub = halo.HaloBatch([g], [ghost.data_ptr()], [p_batch.data_ptr()], unpack=True)
+    ub.launch()
+    halo.unpack_plain(g, p_plain.data_ptr(), ghost2.data_ptr())
+    torch.cuda.synchronize()
+    exp = oracle_unpack(g, want, data_np)
+    assert ghost.cpu().numpy().tobytes() == exp.tobytes()
+    assert ghost2.cpu().numpy().tobytes() == exp.tobytes()
+    b.close()
+    ub.close()
+
+
+def test_graph_replay_sees_new_data(cuda, mpi_init):
+    import torch
+
+    g = halo.Grid((24, 10, 7), 2)
+    data = torch.zeros(g.nbytes, dtype=torch.uint8, device="cuda")
+    packed = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
+    s = torch.cuda.Stream()
+    b = halo.HaloBatch([g], [data.data_ptr()], [packed.data_ptr()])
+    with torch.cuda.stream(s):
+        b.capture(s.cuda_stream)
+    for seed in (1, 2, 3):
+        d_np = H.splitmix_bytes(g.nbytes, seed)
+        data.copy_(torch.from_numpy(d_np))
+        torch.cuda.synchronize()
+        b.replay(s.cuda_stream)
+        s.synchronize()
+        assert packed.cpu().numpy().tobytes() == oracle_pack(g, d_np).tobytes()
+    b.close()
+
+
+def test_mixed_batch_of_8_grids(cuda, mpi_init):
+    """Eight grids with log-uniform interiors and radius 1-3, 208 regions,
+    one launch (config 3's mixed batch at test sizes)."""
+    import torch
+
+    rng = np.random.default_rng(3)
+    grids, datas, packs, nps = [], [], [], []
+    for i in range(8):
+        interior = [int(np.exp(rng.uniform(np.log(4), np.log(24)))) for _ in range(3)]
+        g = halo.Grid(interior, int(rng.integers(1, 4)))
+        d_np = H.splitmix_bytes(g.nbytes, 50 + i)
+        grids.append(g)
+        nps.append(d_np)
+        datas.append(torch.from_numpy(d_np).cuda())
+        packs.append(torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda"))
+    b = halo.HaloBatch(grids, [d.data_ptr() for d in datas], [p.data_ptr() for p in packs])
+    assert b.nregions == 208
+    b.launch()
+    torch.cuda.synchronize()
+    for g, d_np, p in zip(grids, nps, packs):
+        assert p.cpu().numpy().tobytes() == oracle_pack(g, d_np).tobytes()
+    b.close()
+
+
+def test_batch_counts_one_launch(cuda, mpi_init):
+    import torch
+
+    g = halo.Grid((12, 12, 12), 2)
+    data = torch.zeros(g.nbytes, dtype=torch.uint8, device="cuda")
+    packed = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
+    b = halo.HaloBatch([g], [data.data_ptr()], [packed.data_ptr()])
+    n0 = _lib.tempi().tempi_kernel_launches()
+    b.launch()
+    torch.cuda.synchronize()
+    assert _lib.tempi().tempi_kernel_launches() == n0 + 1
+    n0 = _lib.tempi().tempi_kernel_launches()
+    halo.pack_plain(g, data.data_ptr(), packed.data_ptr())
+    assert _lib.tempi().tempi_kernel_launches() == n0 + 26
+    b.close()

@@ -1,0 +1,253 @@
+"""Parity of the CUDA pack/unpack path with the oracle, through the C ABI.
+
+Every check is byte-for-byte.  Unpack destinations are pre-filled with 0xAA
+so that a write to a gap byte shows up as a mismatch (the reference's own
+test pre-fills with the source pattern, test/pack_unpack.cpp:54-57, which
+cannot see such writes).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import types as T
+from oracle import walker as W
+from tempi_b200 import _lib, mpi
+
+from . import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a: np.ndarray):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t) -> np.ndarray:
+    return t.cpu().numpy()
+
+
+def sync():
+    import torch
+
+    torch.cuda.synchronize()
+
+
+def pack_dev(ty, src_np, count, origin=0):
+    """MPI_Pack through the interposer with device buffers."""
+    src = dev(src_np)
+    out = dev(np.zeros(max(ty.o.size * count, 1), np.uint8))
+    sync()
+    err, pos = mpi.Pack(src.data_ptr() + origin, count, ty.h, out.data_ptr(), out.numel())
+    assert err == 0, _lib.last_error()
+    assert pos == ty.o.size * count
+    return host(out)[: pos], src, out
+
+
+def unpack_dev(ty, packed_dev, nbytes, count, origin=0):
+    dst = dev(np.full(nbytes, 0xAA, np.uint8))
+    sync()
+    err, pos = mpi.Unpack(packed_dev.data_ptr(), ty.o.size * count, dst.data_ptr() + origin,
+                          count, ty.h)
+    assert err == 0, _lib.last_error()
+    return host(dst)
+
+
+def check_roundtrip(ty, count, seed=0, pattern=False):
+    o = ty.o
+    lo, hi = H.span(o, count)
+    lo = min(lo, 0)
+    nbytes = hi - lo + 64
+    src = (np.arange(nbytes) & 0xFF).astype(np.uint8) if pattern else H.splitmix_bytes(nbytes, seed)
+    want = W.Walker(o).pack(src, count, origin=-lo, nthreads=8)
+    got, _, out = pack_dev(ty, src, count, origin=-lo)
+    assert got.tobytes() == want.tobytes(), f"pack mismatch {ty.name} x{count}"
+    exp = np.full(nbytes, 0xAA, np.uint8)
+    W.Walker(o).unpack(want, exp, count, origin=-lo, nthreads=8)
+    dst = unpack_dev(ty, out, nbytes, count, origin=-lo)
+    assert dst.tobytes() == exp.tobytes(), f"unpack mismatch {ty.name} x{count}"
+
+
+@pytest.mark.parametrize("case", range(13))
+def test_reference_shapes(cuda, mpi_init, case):
+    """Every shape of the reference's test/pack_unpack.cpp, src[i] = (char)i."""
+    ty, count = H.reference_pack_cases()[case]
+    ty.commit()
+    check_roundtrip(ty, count, pattern=True)
+
+
+def test_config1_device(cuda, mpi_init):
+    ty = H.make_2d_byte_vector(1024, 64, 512).commit()
+    check_roundtrip(ty, 1, seed=0)
+    assert _lib.counter("packs") > 0
+
+
+def test_random_types(cuda, mpi_init):
+    rng = np.random.default_rng(77)
+    done = 0
+    for _ in range(150):
+        ty = H.random_type(rng).commit()
+        if mpi.describe(ty.h)[0] != 0:
+            continue
+        check_roundtrip(ty, int(rng.integers(1, 4)), seed=int(rng.integers(0, 1 << 30)))
+        done += 1
+    assert done > 100
+
+
+def test_golden_fixtures(cuda, mpi_init):
+    import json
+    import os
+
+    gdir = os.path.join(os.path.dirname(__file__), "golden")
+    for f in sorted(x for x in os.listdir(gdir) if x.endswith(".json")):
+        g = json.load(open(os.path.join(gdir, f)))
+        ty = _build_ty(g["type"]).commit()
+        buf = H.splitmix_bytes(g["buf_bytes"], g["seed"])
+        got, _, _ = pack_dev(ty, buf, g["incount"], origin=g["origin"])
+        assert got.tobytes().hex() == g["packed_hex"], f
+
+
+def _build_ty(spec):
+    k = spec["kind"]
+    if k == "named":
+        return H.named({1: "BYTE", 4: "FLOAT", 8: "DOUBLE"}[spec["size"]])
+    c = _build_ty(spec["child"])
+    if k == "vector":
+        return H.vector(spec["count"], spec["bl"], spec["stride"], c)
+    if k == "hvector":
+        return H.hvector(spec["count"], spec["bl"], spec["stride"], c)
+    if k == "contiguous":
+        return H.contiguous(spec["count"], c)
+    if k == "subarray":
+        return H.subarray(spec["sizes"], spec["subsizes"], spec["starts"], spec["order"], c)
+    if k == "resized":
+        return H.resized(c, spec["lb"], spec["extent"])
+    raise ValueError(k)
+
+
+def test_truncation_writes_nothing(cuda, mpi_init):
+    ty = H.make_2d_byte_vector(64, 16, 32).commit()
+    src = dev(H.splitmix_bytes(2048, 3))
+    out = dev(np.full(512, 0x55, np.uint8))
+    sync()
+    err, pos = mpi.Pack(src.data_ptr(), 1, ty.h, out.data_ptr(), 512)
+    assert err == mpi.ERR_TRUNCATE and pos == 0
+    assert (host(out) == 0x55).all()
+    err, pos = mpi.Unpack(out.data_ptr(), 100, src.data_ptr(), 1, ty.h)
+    assert err == mpi.ERR_TRUNCATE
+
+
+def test_positions_accumulate(cuda, mpi_init):
+    """Several packs into one buffer at increasing positions, then unpacks."""
+    a = H.make_2d_byte_vector(8, 5, 9).commit()
+    b = H.subarray([6, 10], [3, 4], [2, 5], mpi.ORDER_C, H.named("FLOAT")).commit()
+    sa, sb = H.splitmix_bytes(a.o.extent * 3, 1), H.splitmix_bytes(b.o.extent * 2, 2)
+    da, db = dev(sa), dev(sb)
+    total = a.o.size * 3 + b.o.size * 2
+    out = dev(np.zeros(total, np.uint8))
+    sync()
+    err, pos = mpi.Pack(da.data_ptr(), 3, a.h, out.data_ptr(), total, 0)
+    assert err == 0
+    err, pos = mpi.Pack(db.data_ptr(), 2, b.h, out.data_ptr(), total, pos)
+    assert err == 0 and pos == total
+    want = np.concatenate([T.pack(a.o, sa, 3), T.pack(b.o, sb, 2)])
+    assert host(out).tobytes() == want.tobytes()
+
+
+def test_pack_into_pinned_host(cuda, mpi_init):
+    """Mapped pinned host memory is device-accessible, so the kernel writes
+    it directly (the ONE_SHOT store path)."""
+    import torch
+
+    ty = H.make_byte_v_hv((12, 7, 5), (40, 20, 10)).commit()
+    src_np = H.splitmix_bytes(ty.o.extent * 2, 4)
+    src = dev(src_np)
+    out = torch.zeros(ty.o.size * 2, dtype=torch.uint8).pin_memory()
+    sync()
+    err, pos = mpi.Pack(src.data_ptr(), 2, ty.h, out.data_ptr(), out.numel())
+    assert err == 0
+    assert out.numpy().tobytes() == T.pack(ty.o, src_np, 2).tobytes()
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("width", [1, 2, 4, 8, 16])
+@pytest.mark.parametrize("threads", [64, 256, 512])
+def test_kernel_variants(cuda, mpi_init, kernel, width, threads):
+    """Every kernel variant, width and block size writes the same bytes."""
+    import torch
+
+    cases = [
+        _lib.Desc.make(48, 1 << 20, 256, [100, 7], [1024, 1024 * 128]),
+        _lib.Desc.make(16, 112 * 4096, 64, [4096], [64 + 16 * 3]),
+        _lib.Desc.make(0, 8192 * 33, 4096, [33], [4096 * 2]),
+        _lib.Desc.make(32, 1 << 16, 32, [3, 5, 7, 2], [64, 256, 2048, 20000]),
+    ]
+    for d in cases:
+        incount = 3
+        o_span = d.start + d.extent * (incount - 1) + 1
+        for k in range(d.ndims):
+            o_span += d.strides[k] * (d.counts[k] - 1)
+        o_span += d.block + 64
+        src_np = H.splitmix_bytes(o_span, 9)
+        src = dev(src_np)
+        out = torch.zeros(d.size * incount, dtype=torch.uint8, device="cuda")
+        cfg = _lib.Config(kernel, width, threads, 0, 0, 0)
+        _lib.check(_lib.tempi().tempi_pack(ctypes.byref(d), src.data_ptr(), incount,
+                                            out.data_ptr(), ctypes.byref(cfg), None))
+        sync()
+        from tests.test_canon import desc_pack
+
+        want = desc_pack(d, src_np, incount)
+        assert host(out).tobytes() == want.tobytes()
+        back = torch.full_like(src, 0xAA)
+        _lib.check(_lib.tempi().tempi_unpack(ctypes.byref(d), out.data_ptr(), incount,
+                                              back.data_ptr(), ctypes.byref(cfg), None))
+        sync()
+        b = host(back)
+        exp = np.full_like(src_np, 0xAA)
+        v = np.lib.stride_tricks.as_strided(
+            exp[d.start:], shape=[incount] + [d.counts[k] for k in reversed(range(d.ndims))] + [d.block],
+            strides=[d.extent] + [d.strides[k] for k in reversed(range(d.ndims))] + [1], writeable=True)
+        v[...] = want.reshape(v.shape)
+        assert b.tobytes() == exp.tobytes()
+
+
+SWEEP_2D = [(c, 1024) for c in (1, 2, 4, 8, 16, 64, 256, 1024)]
+SWEEP_3D = [(c, 256, 256) for c in (1, 2, 4, 8, 16, 64, 256)]
+
+
+@pytest.mark.parametrize("inner,rows", SWEEP_2D)
+@pytest.mark.parametrize("incount", [1, 16])
+def test_sweep_2d_full_size(cuda, mpi_init, inner, rows, incount):
+    """Benchmark config 2, 2-D: float subarrays of a 1024x1024 array at full
+    size, starts from a seed, compared with the oracle's C walker."""
+    rng = np.random.default_rng(inner * 31 + incount)
+    sc = int(rng.integers(0, 1024 - inner + 1))
+    ty = H.subarray([1024, 1024], [rows, inner], [0, sc], mpi.ORDER_C, H.named("FLOAT")).commit()
+    check_roundtrip(ty, incount, seed=inner)
+
+
+@pytest.mark.parametrize("inner,mid,outer", SWEEP_3D)
+def test_sweep_3d_full_size(cuda, mpi_init, inner, mid, outer):
+    rng = np.random.default_rng(inner)
+    s0 = int(rng.integers(0, 256 - inner + 1))
+    ty = H.subarray([256, 256, 256], [outer, mid, inner], [0, 0, s0], mpi.ORDER_C,
+                    H.named("FLOAT")).commit()
+    check_roundtrip(ty, 4 if inner >= 64 else 1, seed=inner + 100)
+
+
+def test_sweep_equivalent_constructors(cuda, mpi_init):
+    """The same pattern as a subarray, an hvector of vectors and a
+    contiguous of hvectors packs identically (config 2's variants)."""
+    C, r, c, sr, sc = 1024, 96, 24, 5, 13
+    sub = H.subarray([1024, C], [r, c], [sr, sc], mpi.ORDER_C, H.named("FLOAT")).commit()
+    hv = H.resized(H.hvector(r, 1, 4 * C, H.vector(1, c, c, H.named("FLOAT"))), 0, 4 * C * 1024).commit()
+    ch = H.contiguous(1, H.hvector(r, c, 4 * C, H.named("FLOAT"))).commit()
+    src = H.splitmix_bytes(4 * C * 1024 + 64, 5)
+    origin = 4 * (sc + sr * C)
+    a, _, _ = pack_dev(sub, src, 1)
+    b, _, _ = pack_dev(hv, src, 1, origin=origin)
+    c_, _, _ = pack_dev(ch, src, 1, origin=origin)
+    assert a.tobytes() == b.tobytes() == c_.tobytes() == T.pack(sub.o, src, 1).tobytes()

@@ -1,0 +1,134 @@
+"""Self-sends of strided device objects through the interposed
+MPI_Send/MPI_Recv/MPI_Isend/MPI_Irecv/MPI_Wait, by each transfer method
+(benchmark config 5 at small sizes).  The reference only checks that these
+complete (test/isend.cu, test/send.cpp); here every received byte is
+compared with the oracle and gap bytes must keep their 0xAA fill."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import types as T
+from tempi_b200 import _lib, mpi
+
+from . import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+METHODS = {"DEVICE": "TEMPI_DATATYPE_DEVICE", "ONESHOT": "TEMPI_DATATYPE_ONESHOT",
+           "STAGED": "TEMPI_DATATYPE_STAGED"}
+
+
+@pytest.fixture
+def method(request):
+    var = METHODS[request.param]
+    os.environ[var] = ""
+    _lib.tempi().tempi_reload_env()
+    yield request.param
+    os.environ.pop(var, None)
+    _lib.tempi().tempi_reload_env()
+
+
+def dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def expected(ty, src, count):
+    exp = np.full_like(src, 0xAA)
+    T.unpack(ty.o, T.pack(ty.o, src, count), exp, count)
+    return exp
+
+
+def types():
+    return [
+        H.vector(300, 3, 17, H.named("BYTE")),
+        H.subarray([40, 30, 20], [10, 12, 6], [3, 4, 5], mpi.ORDER_C, H.named("FLOAT")),
+        H.make_byte_v_hv((64, 9, 5), (128, 16, 8)),
+        H.vector(64, 1024, 2048, H.named("FLOAT")),
+    ]
+
+
+@pytest.mark.parametrize("method", list(METHODS), indirect=True)
+def test_blocking_self_send(cuda, mpi_init, method):
+    import torch
+
+    before = _lib.counter("send_" + method.lower())
+    for ty in types():
+        ty.commit()
+        count = 2
+        src_np = H.splitmix_bytes(ty.o.extent * count, 11)
+        src, dst = dev(src_np), dev(np.full_like(src_np, 0xAA))
+        torch.cuda.synchronize()
+        assert mpi.Send(src.data_ptr(), count, ty.h) == 0, _lib.last_error()
+        err, st = mpi.Recv(dst.data_ptr(), count, ty.h)
+        assert err == 0, _lib.last_error()
+        assert mpi.Get_count(st, ty.h) == count
+        assert dst.cpu().numpy().tobytes() == expected(ty, src_np, count).tobytes(), ty.name
+    assert _lib.counter("send_" + method.lower()) == before + len(types())
+
+
+@pytest.mark.parametrize("method", list(METHODS), indirect=True)
+@pytest.mark.parametrize("recv_first", [True, False])
+def test_nonblocking_self_send(cuda, mpi_init, method, recv_first):
+    import torch
+
+    for ty in types():
+        ty.commit()
+        count = 3
+        src_np = H.splitmix_bytes(ty.o.extent * count, 12)
+        src, dst = dev(src_np), dev(np.full_like(src_np, 0xAA))
+        torch.cuda.synchronize()
+        if recv_first:
+            e1, rr = mpi.Irecv(dst.data_ptr(), count, ty.h, tag=7)
+            e2, rs = mpi.Isend(src.data_ptr(), count, ty.h, tag=7)
+        else:
+            e2, rs = mpi.Isend(src.data_ptr(), count, ty.h, tag=7)
+            e1, rr = mpi.Irecv(dst.data_ptr(), count, ty.h, tag=7)
+        assert (e1, e2) == (0, 0), _lib.last_error()
+        assert rr & 0x40000000 and rs & 0x40000000  # managed requests
+        err, r, st = mpi.Wait(rr)
+        assert err == 0 and r == mpi.REQUEST_NULL, _lib.last_error()
+        err, r, _ = mpi.Wait(rs)
+        assert err == 0 and r == mpi.REQUEST_NULL
+        assert dst.cpu().numpy().tobytes() == expected(ty, src_np, count).tobytes(), ty.name
+
+
+def test_tags_match_in_order(cuda, mpi_init):
+    import torch
+
+    ty = H.vector(50, 4, 9, H.named("BYTE")).commit()
+    a_np, b_np = H.splitmix_bytes(ty.o.extent, 1), H.splitmix_bytes(ty.o.extent, 2)
+    a, b = dev(a_np), dev(b_np)
+    ra, rb = dev(np.full_like(a_np, 0xAA)), dev(np.full_like(a_np, 0xAA))
+    torch.cuda.synchronize()
+    assert mpi.Send(a.data_ptr(), 1, ty.h, tag=1) == 0
+    assert mpi.Send(b.data_ptr(), 1, ty.h, tag=2) == 0
+    assert mpi.Recv(rb.data_ptr(), 1, ty.h, tag=2)[0] == 0
+    assert mpi.Recv(ra.data_ptr(), 1, ty.h, tag=1)[0] == 0
+    assert ra.cpu().numpy().tobytes() == expected(ty, a_np, 1).tobytes()
+    assert rb.cpu().numpy().tobytes() == expected(ty, b_np, 1).tobytes()
+
+
+def test_wait_without_sender_times_out(cuda, mpi_init):
+    """Failure detection without a GPU fault: a receive whose send never
+    comes makes MPI_Wait return an error after TEMPI_WAIT_TIMEOUT_S instead
+    of spinning forever; the context stays usable afterwards."""
+    import torch
+
+    os.environ["TEMPI_WAIT_TIMEOUT_S"] = "0.5"
+    _lib.tempi().tempi_reload_env()
+    try:
+        ty = H.vector(20, 2, 5, H.named("BYTE")).commit()
+        dst = dev(np.zeros(ty.o.extent, np.uint8))
+        err, rr = mpi.Irecv(dst.data_ptr(), 1, ty.h, tag=99)
+        assert err == 0
+        err, r, _ = mpi.Wait(rr)
+        assert err == mpi.ERR_OTHER and r == mpi.REQUEST_NULL
+        assert "gave up" in _lib.last_error()
+    finally:
+        os.environ.pop("TEMPI_WAIT_TIMEOUT_S")
+        _lib.tempi().tempi_reload_env()
+    # still usable
+    test_tags_match_in_order(torch.device("cuda"), mpi_init)
