@@ -20,7 +20,7 @@ HEADER = os.path.join(ROOT, "include", "tempi_b200.h")
 
 def header_symbols():
     text = open(HEADER).read()
-    funcs = set(re.findall(r"^\s*(?:int|int64_t|const char \*)\s*(tempi_\w+)\(", text, re.M))
+    funcs = set(re.findall(r"^\s*(?:int|int64_t|const char \*|void \*)\s*(tempi_\w+)\(", text, re.M))
     mpis = set(re.findall(r"^\s+(MPI_\w+)\s+replaces", text, re.M))
     return funcs, mpis
 
