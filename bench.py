@@ -250,8 +250,20 @@ class GpuSweep:
         self.alg_bytes = sum(4 * p["size"] * p["incount"] for p in self.pts)
 
     def flush_l2(self, stream):
-        with self.torch.cuda.stream(stream):
-            self.flush.fill_(1)
+        """Write, then read back, a buffer larger than L2 (clean lines)."""
+        driver().tempi_bench_flush(self.flush.data_ptr(), self.flush.numel(),
+                                   stream.cuda_stream)
+
+    def ops(self):
+        """One step: MPI_Pack then MPI_Unpack of every sweep point."""
+        out = []
+        cap = self.packed.numel()
+        for p in self.pts:
+            out.append(BenchOp(0, p["t"], p["src"].data_ptr(), self.packed.data_ptr(),
+                               p["incount"], 0, cap, 0))
+            out.append(BenchOp(1, p["t"], p["dst"].data_ptr(), self.packed.data_ptr(),
+                               p["incount"], 0, cap, 0))
+        return out
 
     def step(self, mpi):
         packed = self.packed.data_ptr()
@@ -313,11 +325,14 @@ def halo_bench(torch, stream, reps=20):
     data = torch.randint(0, 256, (g.nbytes,), dtype=torch.uint8, device="cuda")
     packed = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
-    tstream = torch.cuda.ExternalStream(_tempi_stream())
-    plain = lambda: halo.pack_plain(g, data.data_ptr(), packed.data_ptr())
-    for _ in range(3):
-        plain()
-    t_plain = time_events(torch, tstream, plain, reps)
+    plain_ops = []
+    pos = 0
+    for d in halo.directions():
+        plain_ops.append(BenchOp(0, g.send[d], data.data_ptr(), packed.data_ptr(), 1, pos,
+                                 g.packed_bytes, 0))
+        pos += g.region_bytes[d]
+    run_ops(plain_ops, 3)
+    t_plain = sum(run_ops(plain_ops, reps)) / reps
     b = halo.HaloBatch([g], [data.data_ptr()], [packed.data_ptr()])
     s = stream.cuda_stream
     for _ in range(3):
@@ -343,12 +358,15 @@ def halo_bench(torch, stream, reps=20):
         mb.replay(s)
     t_mixed = time_events(torch, stream, lambda: mb.replay(s), reps)
 
-    def mixed_plain():
-        for gg, d, p in zip(grids, datas, packs):
-            halo.pack_plain(gg, d.data_ptr(), p.data_ptr())
-
-    mixed_plain()
-    t_mixed_plain = time_events(torch, tstream, mixed_plain, 5)
+    mixed_ops = []
+    for gg, dd, pp in zip(grids, datas, packs):
+        pos = 0
+        for d in halo.directions():
+            mixed_ops.append(BenchOp(0, gg.send[d], dd.data_ptr(), pp.data_ptr(), 1, pos,
+                                     gg.packed_bytes, 0))
+            pos += gg.region_bytes[d]
+    run_ops(mixed_ops, 2)
+    t_mixed_plain = sum(run_ops(mixed_ops, 5)) / 5
     mb.close()
     del datas, packs
     return {
@@ -367,6 +385,46 @@ def _tempi_stream():
     from tempi_b200 import _lib
 
     return _lib.tempi().tempi_stream()
+
+
+class BenchOp(ctypes.Structure):
+    """``tempi_bench_op`` of tempi_b200/csrc/bench/driver.cu."""
+
+    _fields_ = [("unpack", ctypes.c_int), ("datatype", ctypes.c_int),
+                ("typed", ctypes.c_void_p), ("packed", ctypes.c_void_p),
+                ("incount", ctypes.c_int), ("position", ctypes.c_int),
+                ("capacity", ctypes.c_int), ("reserved", ctypes.c_int)]
+
+
+_driver = None
+
+
+def driver():
+    """The C benchmark driver (MPI call loops run from C)."""
+    global _driver
+    if _driver is None:
+        from tempi_b200 import _lib
+
+        _lib.tempi()
+        _driver = ctypes.CDLL(os.path.join(ROOT, "tempi_b200", "csrc", "libtempi_bench.so"))
+        _driver.tempi_bench_flush.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        _driver.tempi_bench_mpi_ops.argtypes = [
+            ctypes.POINTER(BenchOp), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+            ctypes.c_size_t, ctypes.POINTER(ctypes.c_float)]
+    return _driver
+
+
+def run_ops(ops, iters, flush=None):
+    """Device ms of each of `iters` passes over `ops` (C loop)."""
+    arr = (BenchOp * len(ops))(*ops)
+    out = (ctypes.c_float * max(iters, 1))()
+    fp, fb = (flush.data_ptr(), flush.numel()) if flush is not None else (None, 0)
+    err = driver().tempi_bench_mpi_ops(arr, len(ops), iters, fp, fb, out)
+    if err:
+        from tempi_b200 import _lib
+
+        raise RuntimeError(f"MPI call failed in the benchmark loop: {err} {_lib.last_error()}")
+    return list(out)[:iters]
 
 
 def e2e_bench(torch, sw, mpi, steps, warmup):
@@ -433,8 +491,8 @@ def run_ours(args):
     sw = GpuSweep(torch, mpi, dev)
     tstream = torch.cuda.ExternalStream(_tempi_stream())
     torch.cuda.synchronize()
-    for _ in range(args.warmup):
-        sw.step(mpi)
+    ops = sw.ops()
+    run_ops(ops, args.warmup, sw.flush)
     torch.cuda.synchronize()
 
     def barrier():
@@ -443,18 +501,9 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     launches0 = lib.tempi_kernel_launches()
-    times = []
     barrier()
     with Clocks(local) as clk:
-        for _ in range(args.steps):
-            sw.flush_l2(tstream)
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(tstream)
-            sw.step(mpi)
-            b.record(tstream)
-            b.synchronize()
-            times.append(a.elapsed_time(b))
+        times = run_ops(ops, args.steps, sw.flush)
     barrier()
     launches = lib.tempi_kernel_launches() - launches0
     ms = sum(times) / len(times)
@@ -464,6 +513,12 @@ def run_ours(args):
         ms = float(t.item())
     value = world * sw.alg_bytes / ms / 1e6  # GB/s over all replicas
 
+    if args.no_extras:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": round(value, 3), "unit": "GB/s",
+                              "ms_per_step": round(ms, 4), "gpu_launches": int(launches),
+                              "note": "--no-extras run (launch-list capture)"}))
+        return
     side = torch.cuda.Stream()
     table = kernel_table(torch, sw, side, lib)
     total_t = sum(r["pack_ms"] + r["unpack_ms"] for r in table)
@@ -500,6 +555,41 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile(args):
+    """A small case for ncu: one sweep point's pack (or unpack) kernel,
+    launched --profile-reps times through tempi_pack/tempi_unpack."""
+    import torch
+
+    from tempi_b200 import _lib, mpi
+
+    assert mpi.Init() == 0
+    lib = _lib.tempi()
+    pt = [p for p in sweep_points() if p[0] == args.profile_point]
+    if not pt:
+        raise SystemExit(f"unknown point {args.profile_point}")
+    label, sizes, subs, starts, _ = pt[0]
+    t = mpi.Type_create_subarray(sizes, subs, starts, mpi.ORDER_C, mpi.FLOAT)
+    assert mpi.Type_commit(t) == 0
+    err, d = mpi.describe(t)
+    assert err == 0
+    n = args.profile_incount
+    src = torch.randint(0, 256, (d.extent * n,), dtype=torch.uint8, device="cuda")
+    dst = torch.zeros_like(src)
+    packed = torch.zeros(d.size * n, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(args.profile_reps):
+        if args.profile_unpack:
+            _lib.check(lib.tempi_unpack(ctypes.byref(d), packed.data_ptr(), n, dst.data_ptr(),
+                                        None, None))
+        else:
+            _lib.check(lib.tempi_pack(ctypes.byref(d), src.data_ptr(), n, packed.data_ptr(),
+                                      None, None))
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_point": label, "incount": n, "packed_bytes": d.size * n,
+                      "kernel": lib.tempi_last_kernel().decode(),
+                      "device_bytes": int(src.numel() * 2 + packed.numel())}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -508,8 +598,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="time the sweep only (for launch-list captures)")
+    ap.add_argument("--profile-point", default=None,
+                    help="run only this sweep point's pack kernel (for ncu)")
+    ap.add_argument("--profile-incount", type=int, default=2)
+    ap.add_argument("--profile-reps", type=int, default=3)
+    ap.add_argument("--profile-unpack", action="store_true")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_point:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -71,8 +71,10 @@ typedef struct tempi_desc {
 } tempi_desc;
 
 /* Kernel choice for one launch.  Zero fields mean "let the library pick".
-   kernel: 0 auto, 1 word kernel, 2 row kernel.  width: vector bytes
-   (1,2,4,8,16; never above what the alignment proof allows). */
+   kernel: 0 auto, 1 word kernel (a thread per vector word), 2 row kernel (a
+   warp per row), 3 shift kernel (a group of `unroll` = 8/16/32 lanes per
+   row, 16-B accesses at any alignment).  width: vector bytes for kernels 1
+   and 2 (1,2,4,8,16; never above what the alignment proof allows). */
 typedef struct tempi_config {
   int32_t kernel;
   int32_t width;

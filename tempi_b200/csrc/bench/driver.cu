@@ -1,0 +1,95 @@
+// Benchmark driver: runs sequences of interposed MPI_Pack / MPI_Unpack calls
+// from C, the way the reference's bin/bench_mpi_pack.cpp drives them, so the
+// measured per-call cost is the library's and not a scripting layer's.
+// Linked against libtempi_b200.so, so MPI_Pack/MPI_Unpack here resolve to
+// the interposed entry points.  Device time per pass comes from CUDA events
+// recorded on TEMPI's own stream (tempi_stream()), which every interposed
+// call launches on and synchronises.
+#include <mpi.h>
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "tempi_b200.h"
+
+namespace {
+
+// read every 16-B word of `buf` so the L2 holds clean lines afterwards
+__global__ void read_all(const uint4 *__restrict__ buf, size_t n,
+                         unsigned *__restrict__ sink) {
+  unsigned acc = 0;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x) {
+    uint4 v = __ldcg(buf + i);
+    acc ^= v.x ^ v.y ^ v.z ^ v.w;
+  }
+  if (acc == 0x9e3779b9u)
+    *sink = acc; // practically never taken; keeps the loads alive
+}
+
+unsigned *g_sink = nullptr;
+
+} // namespace
+
+extern "C" {
+
+typedef struct tempi_bench_op {
+  int unpack; // 0: MPI_Pack(typed -> packed), 1: MPI_Unpack(packed -> typed)
+  int datatype;
+  void *typed;
+  void *packed;
+  int incount;
+  int position;
+  int capacity;
+  int reserved;
+} tempi_bench_op;
+
+// Evict the L2: write `bytes` of `buf`, then read them back so that the
+// lines left behind are clean (a dirty L2 would bill its write-back to the
+// next timed kernel).
+int tempi_bench_flush(void *buf, size_t bytes, void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!g_sink && cudaMalloc(&g_sink, sizeof(unsigned)) != cudaSuccess)
+    return 2;
+  if (cudaMemsetAsync(buf, 1, bytes, s) != cudaSuccess)
+    return 2;
+  read_all<<<1184, 256, 0, s>>>(static_cast<const uint4 *>(buf), bytes / 16,
+                                g_sink);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// Run `iters` passes over `ops`; ms_out[i] is pass i's device time.  With
+// `flush` non-null the L2 is flushed (untimed) before each pass.
+int tempi_bench_mpi_ops(const tempi_bench_op *ops, int n, int iters,
+                        void *flush, size_t flush_bytes, float *ms_out) {
+  cudaStream_t s = static_cast<cudaStream_t>(tempi_stream());
+  cudaEvent_t a, b;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess)
+    return 2;
+  int err = 0;
+  for (int it = 0; it < iters && !err; ++it) {
+    if (flush && tempi_bench_flush(flush, flush_bytes, s))
+      err = 2;
+    cudaEventRecord(a, s);
+    for (int i = 0; i < n && !err; ++i) {
+      const tempi_bench_op &o = ops[i];
+      int pos = o.position;
+      err = o.unpack ? MPI_Unpack(o.packed, o.capacity, &pos, o.typed,
+                                  o.incount, o.datatype, MPI_COMM_WORLD)
+                     : MPI_Pack(o.typed, o.incount, o.datatype, o.packed,
+                                o.capacity, &pos, MPI_COMM_WORLD);
+    }
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms_out)
+      ms_out[it] = ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return err;
+}
+
+} // extern "C"

@@ -140,7 +140,99 @@ __global__ void __launch_bounds__(512)
   }
 }
 
+// Row copy for rows whose source and destination disagree modulo 16.
+// Each group of L lanes owns one row.  Destination bytes are written as
+// 16-B aligned words (head and tail bytes singly); the source is read as the
+// 16-B aligned words that cover it, and each destination word is assembled
+// from two neighbouring source words with funnel shifts.  A lane loads one
+// source word and takes the next from its neighbour with a shuffle, so every
+// source byte is loaded once.  Aligned 16-B reads that stick out past either
+// end of a row stay inside the 16-B chunk holding a row byte, so they never
+// leave the row's memory page; their extra bytes are discarded.
+template <int L>
+__device__ __forceinline__ void shifted_row(const char *__restrict__ s,
+                                            char *__restrict__ d, uint32_t n,
+                                            uint32_t lane) {
+  const uint32_t head =
+      min(n, uint32_t((16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15));
+  for (uint32_t i = lane; i < head; i += L)
+    d[i] = s[i];
+  const uint32_t nb = (n - head) >> 4; // whole destination words
+  const uint32_t tail0 = head + (nb << 4);
+  for (uint32_t i = tail0 + lane; i < n; i += L)
+    d[i] = s[i];
+  if (nb == 0)
+    return;
+  const char *sa = s + head;
+  uint4 *dw = reinterpret_cast<uint4 *>(d + head);
+  const uint32_t o = reinterpret_cast<uintptr_t>(sa) & 15;
+  const uint4 *aw = reinterpret_cast<const uint4 *>(sa - o);
+  if (o == 0) {
+    for (uint32_t j = lane; j < nb; j += L)
+      dw[j] = __ldg(aw + j);
+    return;
+  }
+  const uint32_t q = o >> 2, sh = (o & 3) * 8;
+  constexpr unsigned kMask = L == 32 ? 0xffffffffu : ((1u << L) - 1u);
+  const unsigned mask = kMask << (threadIdx.x & 31 & ~(L - 1));
+  // all lanes of a group run the same number of iterations
+  for (uint32_t base = 0; base < nb; base += L) {
+    const uint32_t j = base + lane;
+    uint4 a = make_uint4(0, 0, 0, 0);
+    if (j <= nb)
+      a = __ldg(aw + j);
+    uint4 b;
+    b.x = __shfl_down_sync(mask, a.x, 1, L);
+    b.y = __shfl_down_sync(mask, a.y, 1, L);
+    b.z = __shfl_down_sync(mask, a.z, 1, L);
+    b.w = __shfl_down_sync(mask, a.w, 1, L);
+    if (lane == L - 1 && j + 1 <= nb)
+      b = __ldg(aw + j + 1);
+    if (j < nb) {
+      // the five 32-bit source words that cover destination word j
+      uint32_t x0, x1, x2, x3, x4;
+      switch (q) {
+      case 0: x0 = a.x, x1 = a.y, x2 = a.z, x3 = a.w, x4 = b.x; break;
+      case 1: x0 = a.y, x1 = a.z, x2 = a.w, x3 = b.x, x4 = b.y; break;
+      case 2: x0 = a.z, x1 = a.w, x2 = b.x, x3 = b.y, x4 = b.z; break;
+      default: x0 = a.w, x1 = b.x, x2 = b.y, x3 = b.z, x4 = b.w; break;
+      }
+      dw[j] = make_uint4(__funnelshift_r(x0, x1, sh), __funnelshift_r(x1, x2, sh),
+                         __funnelshift_r(x2, x3, sh), __funnelshift_r(x3, x4, sh));
+    }
+  }
+}
+
+template <int L, int ND, bool UNPACK>
+__global__ void __launch_bounds__(256)
+    k_rows_shift(char *__restrict__ strided, char *__restrict__ packed,
+                 const __grid_constant__ Geometry g) {
+  const uint32_t lane = threadIdx.x & (L - 1);
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) / L;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) / L;
+  const uint32_t n = uint32_t(g.block);
+  for (uint32_t row = group; row < g.rows; row += ngroups) {
+    char *s = strided + row_offset<ND>(row, g);
+    char *p = packed + int64_t(row) * g.block;
+    if (UNPACK)
+      shifted_row<L>(p, s, n, lane);
+    else
+      shifted_row<L>(s, p, n, lane);
+  }
+}
+
 using KernelFn = void (*)(char *, char *, Geometry);
+
+template <int L, bool UNPACK> KernelFn pick_shift(uint32_t nd) {
+  switch (nd) {
+  case 0: return k_rows_shift<L, 0, UNPACK>;
+  case 1: return k_rows_shift<L, 1, UNPACK>;
+  case 2: return k_rows_shift<L, 2, UNPACK>;
+  case 3: return k_rows_shift<L, 3, UNPACK>;
+  case 4: return k_rows_shift<L, 4, UNPACK>;
+  default: return k_rows_shift<L, 5, UNPACK>;
+  }
+}
 
 template <int W, bool UNPACK> KernelFn pick_words(uint32_t nd) {
   switch (nd) {
@@ -165,6 +257,13 @@ template <int W, bool UNPACK> KernelFn pick_rows(uint32_t nd) {
 }
 
 template <bool UNPACK> KernelFn pick(int kernel, uint32_t width, uint32_t nd) {
+  if (kernel == 3) { // `width` carries the lanes per row here
+    switch (width) {
+    case 8: return pick_shift<8, UNPACK>(nd);
+    case 16: return pick_shift<16, UNPACK>(nd);
+    default: return pick_shift<32, UNPACK>(nd);
+    }
+  }
   if (kernel == 2) {
     switch (width) {
     case 16: return pick_rows<16, UNPACK>(nd);
@@ -184,16 +283,17 @@ template <bool UNPACK> KernelFn pick(int kernel, uint32_t width, uint32_t nd) {
 }
 
 static const char *kernel_name(int kernel, uint32_t width, bool unpack) {
-  static char names[2][2][17][32];
+  static char names[3][2][33][32];
   static std::once_flag once;
   std::call_once(once, [] {
-    for (int k = 0; k < 2; ++k)
+    const char *k_names[3] = {"words", "rows", "shift"};
+    for (int k = 0; k < 3; ++k)
       for (int u = 0; u < 2; ++u)
-        for (int w = 1; w <= 16; w *= 2)
-          std::snprintf(names[k][u][w], 32, "%s_%s_w%d",
-                        k ? "rows" : "words", u ? "unpack" : "pack", w);
+        for (int w = 1; w <= 32; w *= 2)
+          std::snprintf(names[k][u][w], 32, "%s_%s_%s%d", k_names[k],
+                        u ? "unpack" : "pack", k == 2 ? "l" : "w", w);
   });
-  return names[kernel == 2][unpack][width];
+  return names[kernel - 1][unpack][width];
 }
 
 int num_sms() {
@@ -305,28 +405,45 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
                     cudaStream_t stream) {
   const int sms = num_sms();
   int kernel = cfg ? cfg->kernel : 0;
-  if (kernel != 1 && kernel != 2)
-    kernel = (g.wpr >= 64 && g.rows >= uint32_t(2 * sms)) ? 2 : 1;
+  if (kernel < 1 || kernel > 3) {
+    if (g.width < 16 && g.block >= 128 && g.rows >= uint32_t(sms))
+      kernel = 3; // misaligned wide rows: realign with funnel shifts
+    else if (g.wpr >= 64 && g.rows >= uint32_t(2 * sms))
+      kernel = 2;
+    else
+      kernel = 1;
+  }
+  // rows per group of lanes for the shift kernel
+  uint32_t lanes = 32;
+  if (kernel == 3) {
+    const int req = cfg ? cfg->unroll : 0; // reused: lanes per row
+    lanes = (req == 8 || req == 16 || req == 32)
+                ? uint32_t(req)
+                : (g.block >= 512 ? 32u : g.block >= 256 ? 16u : 8u);
+  }
   int threads = (cfg && cfg->threads) ? cfg->threads : 256;
-  threads = std::max(32, std::min(512, threads / 32 * 32));
+  threads = std::max(32, std::min(kernel == 3 ? 256 : 512, threads / 32 * 32));
   int bps = (cfg && cfg->blocks_per_sm) ? cfg->blocks_per_sm : 2048 / threads;
   int64_t need;
   if (kernel == 2)
     need = (int64_t(g.rows) * 32 + threads - 1) / threads;
+  else if (kernel == 3)
+    need = (int64_t(g.rows) * lanes + threads - 1) / threads;
   else
     need = (int64_t(g.total_words) + int64_t(threads) * kUnroll - 1) /
            (int64_t(threads) * kUnroll);
   int64_t blocks = std::min<int64_t>(need, int64_t(sms) * bps);
   blocks = std::max<int64_t>(blocks, 1);
-  KernelFn fn = unpack ? pick<true>(kernel, g.width, g.nd)
-                       : pick<false>(kernel, g.width, g.nd);
+  const uint32_t sel = kernel == 3 ? lanes : g.width;
+  KernelFn fn = unpack ? pick<true>(kernel, sel, g.nd)
+                       : pick<false>(kernel, sel, g.nd);
   fn<<<unsigned(blocks), threads, 0, stream>>>(const_cast<char *>(strided),
                                                packed, g);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return cuda_error(e, "pack kernel launch");
   counters().kernel_launches++;
-  set_last_kernel(kernel_name(kernel, g.width, unpack));
+  set_last_kernel(kernel_name(kernel, sel, unpack));
   return TEMPI_OK;
 }
 

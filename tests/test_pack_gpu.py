@@ -214,6 +214,42 @@ def test_kernel_variants(cuda, mpi_init, kernel, width, threads):
         assert b.tobytes() == exp.tobytes()
 
 
+@pytest.mark.parametrize("lanes", [8, 16, 32])
+def test_shift_kernel_every_misalignment(cuda, mpi_init, lanes):
+    """The funnel-shift row kernel (kernel 3) at every source and packed
+    misalignment 0..15 and row lengths around the 16-B word boundaries."""
+    import torch
+
+    from tests.test_canon import desc_pack
+
+    for block in (1, 15, 16, 17, 31, 33, 100, 255, 256, 257, 1000):
+        for mis in (0, 1, 2, 3, 4, 5, 7, 8, 9, 12, 13, 15):
+            d = _lib.Desc.make(mis, 64 * 1024, block, [9, 3], [block + 37, 16 * 1024 + 3])
+            incount = 2
+            src_np = H.splitmix_bytes(d.extent * incount + 64, block * 16 + mis)
+            src = dev(src_np)
+            pmis = (mis * 7) % 16  # also misalign the packed side
+            out = torch.zeros(d.size * incount + 32, dtype=torch.uint8, device="cuda")
+            cfg = _lib.Config(3, 0, 128, lanes, 0, 0)
+            _lib.check(_lib.tempi().tempi_pack(ctypes.byref(d), src.data_ptr(), incount,
+                                                out.data_ptr() + pmis, ctypes.byref(cfg), None))
+            sync()
+            want = desc_pack(d, src_np, incount)
+            got = host(out)[pmis: pmis + d.size * incount]
+            assert got.tobytes() == want.tobytes(), (block, mis, lanes)
+            back = torch.full_like(src, 0xAA)
+            _lib.check(_lib.tempi().tempi_unpack(ctypes.byref(d), out.data_ptr() + pmis, incount,
+                                                  back.data_ptr(), ctypes.byref(cfg), None))
+            sync()
+            exp = np.full_like(src_np, 0xAA)
+            v = np.lib.stride_tricks.as_strided(
+                exp[d.start:], shape=[incount, 3, 9, block],
+                strides=[d.extent, d.strides[1], d.strides[0], 1], writeable=True)
+            v[...] = want.reshape(v.shape)
+            assert host(back).tobytes() == exp.tobytes(), (block, mis, lanes)
+            assert _lib.tempi().tempi_last_kernel().decode() == f"shift_unpack_l{lanes}"
+
+
 SWEEP_2D = [(c, 1024) for c in (1, 2, 4, 8, 16, 64, 256, 1024)]
 SWEEP_3D = [(c, 256, 256) for c in (1, 2, 4, 8, 16, 64, 256)]
 
