@@ -506,6 +506,9 @@ def run_ours(args):
         times = run_ops(ops, args.steps, sw.flush)
     barrier()
     launches = lib.tempi_kernel_launches() - launches0
+    if launches < len(ops) * args.steps:
+        raise RuntimeError(f"only {launches} TEMPI kernel launches in the timed region: "
+                           "the MPI calls did not reach the interposer's GPU path")
     ms = sum(times) / len(times)
     if dist is not None:
         t = torch.tensor([ms], device=dev)

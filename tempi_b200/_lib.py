@@ -1,9 +1,12 @@
 """Loads the native libraries and declares their C signatures.
 
-``libminimpi.so`` (the self-only MPI library standing in for the system MPI)
-is loaded first and globally, then ``libtempi_b200.so`` (the interposer and
-its kernels).  Calls through ``tempi()`` reach the interposed MPI entry
-points; calls through ``minimpi()`` reach the underlying library directly.
+``libtempi_b200.so`` (the interposer and its kernels) is loaded globally
+first and ``libminimpi.so`` (the self-only MPI library standing in for the
+system MPI) after it: the order an application gets by linking
+``-ltempi_b200 -lmpi``.  Any library loaded later that calls MPI_Pack binds
+to the interposer, and the interposer reaches the library's MPI_Pack with
+dlsym(RTLD_NEXT).  Calls through ``minimpi()`` reach the underlying library
+directly.
 
 There is no fallback: if a library is missing this raises, telling the user
 to build it.
@@ -183,6 +186,13 @@ def minimpi():
     """The underlying (self-only) MPI library."""
     global _minimpi
     if _minimpi is None:
+        tempi()
+    return _minimpi
+
+
+def _load_minimpi():
+    global _minimpi
+    if _minimpi is None:
         if not os.path.exists(MINIMPI_SO):
             raise ImportError(
                 f"{MINIMPI_SO} is missing: build it with `make -C tempi_b200/csrc`"
@@ -196,15 +206,15 @@ def tempi():
     """libtempi_b200.so: the interposed MPI entry points and the kernel ABI."""
     global _tempi
     if _tempi is None:
-        minimpi()
         if not os.path.exists(TEMPI_SO):
             raise ImportError(
                 f"{TEMPI_SO} is missing: build it with `make -C tempi_b200/csrc`"
             )
-        os.environ.setdefault("TEMPI_LIBMPI", MINIMPI_SO)
-        _tempi = ctypes.CDLL(TEMPI_SO, mode=ctypes.RTLD_GLOBAL)
-        _declare(_tempi, {k: v for k, v in _MPI_SIGS.items() if k in INTERPOSED})
-        _declare(_tempi, _TEMPI_SIGS, required=False)
+        lib = ctypes.CDLL(TEMPI_SO, mode=ctypes.RTLD_GLOBAL)
+        _declare(lib, {k: v for k, v in _MPI_SIGS.items() if k in INTERPOSED})
+        _declare(lib, _TEMPI_SIGS, required=False)
+        _load_minimpi()
+        _tempi = lib
     return _tempi
 
 

@@ -406,7 +406,7 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
   const int sms = num_sms();
   int kernel = cfg ? cfg->kernel : 0;
   if (kernel < 1 || kernel > 3) {
-    if (g.width < 16 && g.block >= 128 && g.rows >= uint32_t(sms))
+    if (!unpack && g.width < 16 && g.block >= 128 && g.rows >= uint32_t(sms))
       kernel = 3; // misaligned wide rows: realign with funnel shifts
     else if (g.wpr >= 64 && g.rows >= uint32_t(2 * sms))
       kernel = 2;

@@ -134,3 +134,23 @@ def test_env_disable_and_no_pack(tmp_path):
                            env=env, timeout=120)
         assert r.returncode == 0, r.stderr
         assert r.stdout.strip() == want, (var, r.stdout)
+
+
+def test_global_scope_binds_mpi_pack_to_the_interposer():
+    """Loaded in link order, any later library's MPI_Pack reaches TEMPI,
+    and TEMPI's dlsym(RTLD_NEXT) reaches the library's."""
+    import ctypes
+
+    _lib.tempi()
+
+    class DlInfo(ctypes.Structure):
+        _fields_ = [("fname", ctypes.c_char_p), ("fbase", ctypes.c_void_p),
+                    ("sname", ctypes.c_char_p), ("saddr", ctypes.c_void_p)]
+
+    libc = ctypes.CDLL(None)
+    glob = ctypes.CDLL(None, mode=os.RTLD_NOW)
+    for name in _lib.INTERPOSED:
+        addr = ctypes.cast(getattr(glob, name), ctypes.c_void_p).value
+        info = DlInfo()
+        assert libc.dladdr(ctypes.c_void_p(addr), ctypes.byref(info))
+        assert info.fname.decode().endswith("libtempi_b200.so"), name
