@@ -72,7 +72,7 @@ typedef struct tempi_desc {
 
 /* Kernel choice for one launch.  Zero fields mean "let the library pick".
    kernel: 0 auto, 1 word kernel (a thread per vector word), 2 row kernel (a
-   warp per row), 3 shift kernel (a group of `unroll` = 8/16/32 lanes per
+   warp per row), 3 shift kernel (a group of `unroll` = 4/8/16/32 lanes per
    row, 16-B accesses at any alignment).  width: vector bytes for kernels 1
    and 2 (1,2,4,8,16; never above what the alignment proof allows). */
 typedef struct tempi_config {

@@ -141,18 +141,36 @@ __global__ void __launch_bounds__(512)
 }
 
 // Row copy for rows whose source and destination disagree modulo 16.
-// Each group of L lanes owns one row.  Destination bytes are written as
-// 16-B aligned words (head and tail bytes singly); the source is read as the
-// 16-B aligned words that cover it, and each destination word is assembled
-// from two neighbouring source words with funnel shifts.  A lane loads one
-// source word and takes the next from its neighbour with a shuffle, so every
-// source byte is loaded once.  Aligned 16-B reads that stick out past either
-// end of a row stay inside the 16-B chunk holding a row byte, so they never
-// leave the row's memory page; their extra bytes are discarded.
+// Each group of L lanes owns one row and each lane K consecutive 16-B
+// destination words per pass, so K independent loads are in flight per lane.
+// Destination bytes are written as 16-B aligned words (head and tail bytes
+// singly); the source is read as the 16-B aligned words that cover it, and
+// each destination word is assembled from two neighbouring source words with
+// funnel shifts.  The word after a lane's last one is the next lane's first,
+// passed with a shuffle, so every source byte is loaded once.  Aligned 16-B
+// reads that stick out past either end of a row stay inside a 16-B chunk that
+// holds a row byte, so they never leave the row's memory page; their extra
+// bytes are discarded.
+constexpr int kShiftWords = 4;
+
+__device__ __forceinline__ uint4 realign(const uint4 &a, const uint4 &b,
+                                         uint32_t q, uint32_t sh) {
+  uint32_t x0, x1, x2, x3, x4; // the five 32-bit words covering the output
+  switch (q) {
+  case 0: x0 = a.x, x1 = a.y, x2 = a.z, x3 = a.w, x4 = b.x; break;
+  case 1: x0 = a.y, x1 = a.z, x2 = a.w, x3 = b.x, x4 = b.y; break;
+  case 2: x0 = a.z, x1 = a.w, x2 = b.x, x3 = b.y, x4 = b.z; break;
+  default: x0 = a.w, x1 = b.x, x2 = b.y, x3 = b.z, x4 = b.w; break;
+  }
+  return make_uint4(__funnelshift_r(x0, x1, sh), __funnelshift_r(x1, x2, sh),
+                    __funnelshift_r(x2, x3, sh), __funnelshift_r(x3, x4, sh));
+}
+
 template <int L>
 __device__ __forceinline__ void shifted_row(const char *__restrict__ s,
                                             char *__restrict__ d, uint32_t n,
                                             uint32_t lane) {
+  constexpr int K = kShiftWords;
   const uint32_t head =
       min(n, uint32_t((16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15));
   for (uint32_t i = lane; i < head; i += L)
@@ -168,38 +186,40 @@ __device__ __forceinline__ void shifted_row(const char *__restrict__ s,
   const uint32_t o = reinterpret_cast<uintptr_t>(sa) & 15;
   const uint4 *aw = reinterpret_cast<const uint4 *>(sa - o);
   if (o == 0) {
-    for (uint32_t j = lane; j < nb; j += L)
-      dw[j] = __ldg(aw + j);
+    for (uint32_t base = 0; base < nb; base += L * K) {
+      const uint32_t j0 = base + lane * K;
+      uint4 v[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (j0 + k < nb)
+          v[k] = __ldg(aw + j0 + k);
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (j0 + k < nb)
+          dw[j0 + k] = v[k];
+    }
     return;
   }
   const uint32_t q = o >> 2, sh = (o & 3) * 8;
   constexpr unsigned kMask = L == 32 ? 0xffffffffu : ((1u << L) - 1u);
   const unsigned mask = kMask << (threadIdx.x & 31 & ~(L - 1));
-  // all lanes of a group run the same number of iterations
-  for (uint32_t base = 0; base < nb; base += L) {
-    const uint32_t j = base + lane;
-    uint4 a = make_uint4(0, 0, 0, 0);
-    if (j <= nb)
-      a = __ldg(aw + j);
-    uint4 b;
-    b.x = __shfl_down_sync(mask, a.x, 1, L);
-    b.y = __shfl_down_sync(mask, a.y, 1, L);
-    b.z = __shfl_down_sync(mask, a.z, 1, L);
-    b.w = __shfl_down_sync(mask, a.w, 1, L);
-    if (lane == L - 1 && j + 1 <= nb)
-      b = __ldg(aw + j + 1);
-    if (j < nb) {
-      // the five 32-bit source words that cover destination word j
-      uint32_t x0, x1, x2, x3, x4;
-      switch (q) {
-      case 0: x0 = a.x, x1 = a.y, x2 = a.z, x3 = a.w, x4 = b.x; break;
-      case 1: x0 = a.y, x1 = a.z, x2 = a.w, x3 = b.x, x4 = b.y; break;
-      case 2: x0 = a.z, x1 = a.w, x2 = b.x, x3 = b.y, x4 = b.z; break;
-      default: x0 = a.w, x1 = b.x, x2 = b.y, x3 = b.z, x4 = b.w; break;
-      }
-      dw[j] = make_uint4(__funnelshift_r(x0, x1, sh), __funnelshift_r(x1, x2, sh),
-                         __funnelshift_r(x2, x3, sh), __funnelshift_r(x3, x4, sh));
-    }
+  // every lane of a group runs the same number of passes (uniform `nb`)
+  for (uint32_t base = 0; base < nb; base += L * K) {
+    const uint32_t j0 = base + lane * K;
+    uint4 a[K + 1];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      a[k] = (j0 + k <= nb) ? __ldg(aw + j0 + k) : make_uint4(0, 0, 0, 0);
+    a[K].x = __shfl_down_sync(mask, a[0].x, 1, L);
+    a[K].y = __shfl_down_sync(mask, a[0].y, 1, L);
+    a[K].z = __shfl_down_sync(mask, a[0].z, 1, L);
+    a[K].w = __shfl_down_sync(mask, a[0].w, 1, L);
+    if (lane == L - 1 && j0 + K <= nb)
+      a[K] = __ldg(aw + j0 + K);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (j0 + k < nb)
+        dw[j0 + k] = realign(a[k], a[k + 1], q, sh);
   }
 }
 
@@ -259,6 +279,7 @@ template <int W, bool UNPACK> KernelFn pick_rows(uint32_t nd) {
 template <bool UNPACK> KernelFn pick(int kernel, uint32_t width, uint32_t nd) {
   if (kernel == 3) { // `width` carries the lanes per row here
     switch (width) {
+    case 4: return pick_shift<4, UNPACK>(nd);
     case 8: return pick_shift<8, UNPACK>(nd);
     case 16: return pick_shift<16, UNPACK>(nd);
     default: return pick_shift<32, UNPACK>(nd);
@@ -417,9 +438,13 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
   uint32_t lanes = 32;
   if (kernel == 3) {
     const int req = cfg ? cfg->unroll : 0; // reused: lanes per row
-    lanes = (req == 8 || req == 16 || req == 32)
+    // one pass of a group covers lanes * kShiftWords * 16 bytes of a row
+    lanes = (req == 4 || req == 8 || req == 16 || req == 32)
                 ? uint32_t(req)
-                : (g.block >= 512 ? 32u : g.block >= 256 ? 16u : 8u);
+                : (g.block > 1024 ? 32u
+                   : g.block > 512 ? 16u
+                   : g.block > 256 ? 8u
+                                   : 4u);
   }
   int threads = (cfg && cfg->threads) ? cfg->threads : 256;
   threads = std::max(32, std::min(kernel == 3 ? 256 : 512, threads / 32 * 32));

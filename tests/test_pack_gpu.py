@@ -214,7 +214,7 @@ def test_kernel_variants(cuda, mpi_init, kernel, width, threads):
         assert b.tobytes() == exp.tobytes()
 
 
-@pytest.mark.parametrize("lanes", [8, 16, 32])
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
 def test_shift_kernel_every_misalignment(cuda, mpi_init, lanes):
     """The funnel-shift row kernel (kernel 3) at every source and packed
     misalignment 0..15 and row lengths around the 16-B word boundaries."""
@@ -222,9 +222,9 @@ def test_shift_kernel_every_misalignment(cuda, mpi_init, lanes):
 
     from tests.test_canon import desc_pack
 
-    for block in (1, 15, 16, 17, 31, 33, 100, 255, 256, 257, 1000):
+    for block in (1, 15, 16, 17, 31, 33, 100, 255, 256, 257, 1000, 2100):
         for mis in (0, 1, 2, 3, 4, 5, 7, 8, 9, 12, 13, 15):
-            d = _lib.Desc.make(mis, 64 * 1024, block, [9, 3], [block + 37, 16 * 1024 + 3])
+            d = _lib.Desc.make(mis, 64 * 1024, block, [9, 3], [block + 37, 9 * (block + 37) + 3])
             incount = 2
             src_np = H.splitmix_bytes(d.extent * incount + 64, block * 16 + mis)
             src = dev(src_np)
