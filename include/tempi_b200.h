@@ -125,6 +125,21 @@ int tempi_batch_capture(tempi_batch *b, void *stream);
 int tempi_batch_replay(tempi_batch *b, void *stream);
 int tempi_batch_destroy(tempi_batch *b);
 
+/* Batched pack (unpack != 0: unpack) of `n` regions in one launch on
+   `stream`, allocating nothing.  No counterpart in the reference.  For
+   callers that cannot allocate device memory where they pack -- a step of
+   a latency-critical loop (cudaMalloc can synchronise the whole device), or
+   an application whose memory pool already owns the GPU's memory -- the
+   region table is kept in a fixed array inside the library instead of
+   memory from cudaMalloc.  At most 1024 regions per call (larger n returns
+   TEMPI_ERR_ARG).  Every GPU that loads the library holds that 168 KiB
+   array until exit.  The first call on a device, with that device current,
+   looks up the array's device address, so make it before any stream
+   capture.  All calls share the array: calls whose launches can overlap on
+   the GPU race on it. */
+int tempi_batch_run_static(const tempi_region *regions, int32_t n,
+                           int32_t unpack, void *stream);
+
 /* ---- runtime ------------------------------------------------------------ */
 /* TEMPI's internal non-blocking stream (a cudaStream_t) on which the MPI
    entry points launch (reference kernStream, src/internal/streams.cpp:16-28).

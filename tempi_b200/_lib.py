@@ -160,6 +160,7 @@ _TEMPI_SIGS = {
     "tempi_batch_capture": (c_int, [c_void_p, c_void_p]),
     "tempi_batch_replay": (c_int, [c_void_p, c_void_p]),
     "tempi_batch_destroy": (c_int, [c_void_p]),
+    "tempi_batch_run_static": (c_int, [P(Region), ctypes.c_int32, ctypes.c_int32, c_void_p]),
     "tempi_last_error": (ctypes.c_char_p, []),
     "tempi_kernel_launches": (c_int64, []),
     "tempi_last_kernel": (ctypes.c_char_p, []),

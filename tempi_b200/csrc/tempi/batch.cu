@@ -17,6 +17,7 @@
 #include "internal.hpp"
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 namespace tempi {
@@ -261,6 +262,124 @@ extern "C" int tempi_batch_replay(tempi_batch *b, void *stream) {
     return cuda_error(e, "graph launch");
   if (!b->impl.host.empty())
     counters().kernel_launches++;
+  return TEMPI_OK;
+}
+
+// ---- batched pack without allocation ------------------------------------
+//
+// tempi_batch_create puts the region table in memory it obtains with
+// cudaMalloc.  Some callers cannot allocate device memory where they pack:
+// a halo-exchange step inside a latency-critical loop (cudaMalloc can
+// synchronise the whole device), or an application whose memory pool
+// already owns the GPU's memory, so any further cudaMalloc fails.  For them
+// tempi_batch_run_static keeps the table in the fixed array below instead.
+//
+// The array is a file-scope device variable: every GPU that loads this
+// library holds it (kStaticBatchRegions = 1024 entries of 168 B: 168 KiB) until the
+// process exits.  Host code cannot use the name `g_static_regions` as a
+// device address (it denotes a host-side stand-in), so the first call on
+// each device, with that device current, asks the runtime for the array's
+// device address once (cudaGetSymbolAddress) and every call passes that
+// address to the kernel.  Because of that set-up, the first call on a
+// device should come before any stream capture.  All calls share the one
+// array and it keeps the last call's table; each call rewrites every entry
+// it uses, so nothing needs clearing, but calls whose launches can overlap
+// on the GPU (different streams, no ordering) race on the table.
+constexpr int kStaticBatchRegions = 1024;
+constexpr int kMaxDevices = 64;
+
+static_assert(sizeof(BatchRegion) == 168, "table entry size is documented");
+static __device__ __align__(256) BatchRegion g_static_regions[kStaticBatchRegions];
+
+static std::mutex g_static_mu;
+static BatchRegion *g_static_ptr[kMaxDevices] = {};
+
+static int static_table(BatchRegion **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess)
+    return cuda_error(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices)
+    return set_error(TEMPI_ERR_ARG, "device %d out of range", dev);
+  std::lock_guard<std::mutex> l(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_regions);
+    if (e != cudaSuccess)
+      return cuda_error(e, "cudaGetSymbolAddress of the static region table");
+    g_static_ptr[dev] = static_cast<BatchRegion *>(p);
+  }
+  *out = g_static_ptr[dev];
+  return TEMPI_OK;
+}
+
+extern "C" int tempi_batch_run_static(const tempi_region *regions, int32_t n,
+                                      int32_t unpack, void *stream) {
+  if (n < 0 || (n > 0 && !regions))
+    return set_error(TEMPI_ERR_ARG, "bad batch arguments");
+  if (n > kStaticBatchRegions)
+    return set_error(TEMPI_ERR_ARG,
+                     "tempi_batch_run_static takes at most %d regions, got %d",
+                     kStaticBatchRegions, n);
+  BatchRegion *table = nullptr;
+  int err = static_table(&table);
+  if (err)
+    return err;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // build the table in fixed-size pieces on the stack and copy each piece;
+  // cudaMemcpyAsync from pageable memory returns once the piece is staged,
+  // so the stack buffer can be reused straight away
+  constexpr int kPiece = 32;
+  BatchRegion piece[kPiece];
+  int used = 0, filled = 0;
+  uint64_t chunks = 0;
+  for (int32_t i = 0; i < n; ++i) {
+    const tempi_region &r = regions[i];
+    BatchRegion &br = piece[filled];
+    br = BatchRegion{};
+    char *strided = (char *)r.origin + r.desc.start;
+    bool empty = false;
+    err = make_geometry(&r.desc, r.incount, uintptr_t(strided),
+                        uintptr_t(r.packed), 0, &br.g, &empty);
+    if (err)
+      return err;
+    if (empty)
+      continue;
+    br.strided = strided;
+    br.packed = (char *)r.packed;
+    br.chunk_begin = uint32_t(chunks);
+    chunks += (br.g.total_words + kChunkWords - 1) / kChunkWords;
+    if (chunks > UINT32_MAX)
+      return set_error(TEMPI_ERR_ARG, "batch too large");
+    if (++filled == kPiece || i == n - 1) {
+      cudaError_t e = cudaMemcpyAsync(table + used, piece,
+                                      filled * sizeof(BatchRegion),
+                                      cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess)
+        return cuda_error(e, "static region table upload");
+      used += filled;
+      filled = 0;
+    }
+  }
+  if (filled) { // the last regions were empty ones after a partial piece
+    cudaError_t e = cudaMemcpyAsync(table + used, piece,
+                                    filled * sizeof(BatchRegion),
+                                    cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess)
+      return cuda_error(e, "static region table upload");
+    used += filled;
+  }
+  if (used == 0)
+    return TEMPI_OK;
+  const uint32_t total = uint32_t(chunks);
+  const uint32_t grid =
+      std::max<uint32_t>(1, std::min<uint32_t>(total, num_sms() * 8));
+  k_batch<<<grid, kBatchThreads, 0, s>>>(table, used, total, unpack ? 1 : 0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return cuda_error(e, "static batch launch");
+  counters().kernel_launches++;
+  set_last_kernel(unpack ? "batch_unpack_static" : "batch_pack_static");
   return TEMPI_OK;
 }
 
