@@ -166,6 +166,17 @@ _TEMPI_SIGS = {
     "tempi_last_kernel": (ctypes.c_char_p, []),
     "tempi_counter": (c_int64, [ctypes.c_char_p]),
     "tempi_stream": (c_void_p, []),
+    "tempi_features": (c_int, [P(Desc), c_int64, c_int, c_int, c_void_p]),
+    "tempi_measure": (c_int, [P(Desc), c_int64, c_int, c_int, c_int, c_int, c_void_p]),
+    "tempi_dispatch_load": (c_int, [ctypes.c_char_p, ctypes.c_char_p]),
+    "tempi_dispatch_choose": (c_int, [P(Desc), c_int64, c_int, c_int, c_int, P(c_int),
+                                      P(c_int), c_void_p, c_void_p]),
+    "tempi_mlp_init": (c_int, [c_void_p, c_int, ctypes.c_uint64]),
+    "tempi_mlp_train": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                c_int, ctypes.c_float, ctypes.c_uint64, c_void_p, c_void_p]),
+    "tempi_mlp_predict": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p]),
+    "tempi_mlp_grad": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
+                               c_void_p, c_void_p]),
     "tempi_reload_env": (c_int, []),
 }
 

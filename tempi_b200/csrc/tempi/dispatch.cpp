@@ -1,11 +1,381 @@
-// Method and kernel-configuration choice.  Replaced in part by the learned
-// model in model.cpp; the fixed rules here are its fallback.
+// Dispatch: learned cost model, measured fallback, the restated perf-table
+// selector, and the fixed rules.  See dispatch.hpp.
 
 #include "dispatch.hpp"
 
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <string>
+#include <vector>
+
 namespace tempi {
 
+// the kernel configurations the model scores (outputs 0..7)
+const tempi_config kCandidates[kNumConfigs] = {
+    {1, 0, 256, 0, 0, 0},  // word kernel, 256 threads
+    {1, 0, 512, 0, 0, 0},  // word kernel, 512 threads
+    {1, 0, 128, 0, 0, 0},  // word kernel, 128 threads
+    {2, 0, 256, 0, 0, 0},  // row kernel (warp per row)
+    {3, 0, 256, 4, 0, 0},  // shift kernel, 4 lanes per row
+    {3, 0, 256, 8, 0, 0},  // shift kernel, 8 lanes per row
+    {3, 0, 256, 16, 0, 0}, // shift kernel, 16 lanes per row
+    {3, 0, 256, 32, 0, 0}, // shift kernel, 32 lanes per row
+};
+
+namespace {
+
+float lg(double v) { return v > 0 ? float(std::log2(v)) : 0.f; }
+
+// ---- the learned model ------------------------------------------------------
+
+struct Model {
+  bool loaded = false;
+  int members = 0;
+  float y_mean[TEMPI_MLP_OUT], y_std[TEMPI_MLP_OUT];
+  std::vector<float> params;
+  float *dev_params = nullptr, *dev_x = nullptr, *dev_out = nullptr;
+  std::string source;
+};
+
+struct Table {
+  bool loaded = false;
+  std::vector<double> pp_dev, pp_host, d2h, h2d;
+  std::vector<std::vector<double>> pack_dev, unpack_dev, pack_host, unpack_host;
+};
+
+std::mutex g_mu;
+Model g_model;
+Table g_table;
+int g_forced = -1;
+double g_spread_limit = 0.5; // log2 units: the members disagree by ~41 %
+
+const char kModelMagic[8] = {'T', 'M', 'L', 'P', 'v', '0', '0', '1'};
+const char kTableMagic[8] = {'T', 'T', 'A', 'B', 'v', '0', '0', '1'};
+
+int load_model_file(const std::string &path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f)
+    return TEMPI_ERR_ARG;
+  char magic[8];
+  int32_t dims[4];
+  f.read(magic, 8);
+  f.read(reinterpret_cast<char *>(dims), sizeof(dims));
+  if (!f || std::memcmp(magic, kModelMagic, 8) || dims[0] != TEMPI_MLP_IN ||
+      dims[1] != TEMPI_MLP_HIDDEN || dims[2] != TEMPI_MLP_OUT || dims[3] <= 0 ||
+      dims[3] > 64)
+    return set_error(TEMPI_ERR_ARG, "%s is not a cost model file", path.c_str());
+  Model m;
+  m.members = dims[3];
+  f.read(reinterpret_cast<char *>(m.y_mean), sizeof(m.y_mean));
+  f.read(reinterpret_cast<char *>(m.y_std), sizeof(m.y_std));
+  m.params.resize(size_t(m.members) * TEMPI_MLP_PARAMS);
+  f.read(reinterpret_cast<char *>(m.params.data()),
+         m.params.size() * sizeof(float));
+  if (!f)
+    return set_error(TEMPI_ERR_ARG, "%s is truncated", path.c_str());
+  m.loaded = true;
+  m.source = path;
+  std::lock_guard<std::mutex> l(g_mu);
+  cudaFree(g_model.dev_params);
+  cudaFree(g_model.dev_x);
+  cudaFree(g_model.dev_out);
+  g_model = std::move(m);
+  LOG_INFO("cost model loaded from %s (%d members)", path.c_str(),
+           g_model.members);
+  return TEMPI_OK;
+}
+
+template <class T> bool rd(std::ifstream &f, std::vector<T> &v, size_t n) {
+  v.resize(n);
+  f.read(reinterpret_cast<char *>(v.data()), n * sizeof(T));
+  return bool(f);
+}
+
+int load_table_file(const std::string &path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f)
+    return TEMPI_ERR_ARG;
+  char magic[8];
+  int32_t dims[3];
+  f.read(magic, 8);
+  f.read(reinterpret_cast<char *>(dims), sizeof(dims));
+  if (!f || std::memcmp(magic, kTableMagic, 8) || dims[0] <= 0 ||
+      dims[1] <= 0 || dims[2] <= 0 || dims[0] > 64 || dims[1] > 64 ||
+      dims[2] > 64)
+    return set_error(TEMPI_ERR_ARG, "%s is not a table file", path.c_str());
+  Table t;
+  bool ok = rd(f, t.pp_dev, dims[0]) && rd(f, t.pp_host, dims[0]) &&
+            rd(f, t.d2h, dims[0]) && rd(f, t.h2d, dims[0]);
+  for (auto *tab : {&t.pack_dev, &t.unpack_dev, &t.pack_host, &t.unpack_host}) {
+    tab->resize(dims[1]);
+    for (auto &row : *tab)
+      ok = ok && rd(f, row, dims[2]);
+  }
+  if (!ok)
+    return set_error(TEMPI_ERR_ARG, "%s is truncated", path.c_str());
+  t.loaded = true;
+  std::lock_guard<std::mutex> l(g_mu);
+  g_table = std::move(t);
+  return TEMPI_OK;
+}
+
+// Ensemble prediction (log2 microseconds) for one feature row: the mean
+// over members and the spread (standard deviation) of each output.
+int predict(const float f[TEMPI_MLP_IN], float mean[TEMPI_MLP_OUT],
+            float spread[TEMPI_MLP_OUT]) {
+  std::lock_guard<std::mutex> l(g_mu);
+  Model &m = g_model;
+  if (!m.loaded || !cuda_available())
+    return TEMPI_ERR_UNSUPPORTED;
+  cudaError_t e = cudaSuccess;
+  if (!m.dev_params) {
+    e = cudaMalloc(&m.dev_params, m.params.size() * sizeof(float));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(m.dev_params, m.params.data(),
+                     m.params.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMalloc(&m.dev_x, TEMPI_MLP_IN * sizeof(float));
+    if (e == cudaSuccess)
+      e = cudaMalloc(&m.dev_out, size_t(m.members) * TEMPI_MLP_OUT * sizeof(float));
+    if (e != cudaSuccess)
+      return cuda_error(e, "cost model upload");
+  }
+  cudaStream_t s = pack_stream();
+  float out[64 * TEMPI_MLP_OUT];
+  e = cudaMemcpyAsync(m.dev_x, f, TEMPI_MLP_IN * sizeof(float),
+                      cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess)
+    return cuda_error(e, "cost model input");
+  int err = tempi_mlp_predict(m.dev_params, m.members, m.dev_x, 1, m.dev_out, s);
+  if (err)
+    return err;
+  e = cudaMemcpyAsync(out, m.dev_out,
+                      size_t(m.members) * TEMPI_MLP_OUT * sizeof(float),
+                      cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess)
+    return cuda_error(e, "cost model output");
+  for (int j = 0; j < TEMPI_MLP_OUT; ++j) {
+    double s1 = 0, s2 = 0;
+    for (int k = 0; k < m.members; ++k) {
+      const double v = out[k * TEMPI_MLP_OUT + j] * m.y_std[j] + m.y_mean[j];
+      s1 += v;
+      s2 += v * v;
+    }
+    mean[j] = float(s1 / m.members);
+    spread[j] = float(std::sqrt(std::max(0.0, s2 / m.members - (s1 / m.members) *
+                                                               (s1 / m.members))));
+  }
+  return TEMPI_OK;
+}
+
+// ---- the restated perf-table selector ---------------------------------------
+// Same model as the reference's Performance::model_device / model_oneshot
+// (measure_system.cpp:106-138): pack + transfer + unpack, each interpolated
+// from tables measured on this machine.  1-D tables: entry i is 2^i bytes;
+// 2-D tables: entry [i][j] is 2^(2i+6) bytes packed from blocks of 2^j bytes.
+
+int floor_log2(int64_t x) { return x <= 1 ? 0 : 63 - __builtin_clzll(uint64_t(x)); }
+int ceil_log2(int64_t x) {
+  const int f = floor_log2(x);
+  return (x > 1 && (x & (x - 1))) ? f + 1 : f;
+}
+
+double table_1d(const std::vector<double> &a, int64_t bytes) {
+  if (a.empty())
+    return INFINITY;
+  const int lo = floor_log2(bytes), hi = ceil_log2(bytes);
+  if (hi >= int(a.size())) // beyond the table: scale the last entry linearly
+    return a.back() * double(bytes) / double(int64_t(1) << (a.size() - 1));
+  if (lo == hi)
+    return a[lo];
+  const float f = float(bytes - (int64_t(1) << lo)) /
+                  float((int64_t(1) << hi) - (int64_t(1) << lo));
+  return a[lo] * (1 - f) + a[hi] * f;
+}
+
+double table_2d(const std::vector<std::vector<double>> &a, int64_t bytes,
+                int64_t block) {
+  if (a.empty())
+    return INFINITY;
+  block = std::max<int64_t>(1, std::min<int64_t>(block, 512));
+  const int yi1 = (floor_log2(bytes) - 6) / 2;
+  const int64_t y1 = int64_t(1) << (2 * std::max(yi1, 0) + 6);
+  const int yi2 = y1 == bytes ? yi1 : yi1 + 1;
+  const int64_t y2 = int64_t(1) << (2 * yi2 + 6);
+  int xi1 = floor_log2(block), xi2 = ceil_log2(block);
+  const int rows = int(a.size());
+  const std::vector<double> &ref = a[std::min(std::max(yi2, 0), rows - 1)];
+  xi2 = std::min(xi2, int(ref.size()) - 1);
+  xi1 = std::min(xi1, xi2);
+  const int64_t x1 = int64_t(1) << xi1, x2 = int64_t(1) << xi2;
+  const float sx = xi1 == xi2 ? 0.f : float(block - x1) / float(x2 - x1);
+  const float sy = yi1 == yi2 ? 0.f : float(bytes - y1) / float(y2 - y1);
+  if (yi2 >= rows) {
+    const std::vector<double> &last = a.back();
+    const double base = (1 - sx) * last[xi1] + sx * last[xi2];
+    const double ymax = double(int64_t(1) << (2 * (rows - 1) + 6));
+    return base / ymax * double(bytes);
+  }
+  const int r1 = std::max(yi1, 0);
+  const double f1 = (1 - sx) * a[r1][xi1] + sx * a[r1][xi2];
+  const double f2 = (1 - sx) * a[yi2][xi1] + sx * a[yi2][xi2];
+  return (1 - sy) * f1 + sy * f2;
+}
+
+Method table_method(int64_t bytes, int64_t block) {
+  std::lock_guard<std::mutex> l(g_mu);
+  const Table &t = g_table;
+  const double dev = table_2d(t.pack_dev, bytes, block) +
+                     table_1d(t.pp_dev, bytes) +
+                     table_2d(t.unpack_dev, bytes, block);
+  const double one = table_2d(t.pack_host, bytes, block) +
+                     table_1d(t.pp_host, bytes) +
+                     table_2d(t.unpack_host, bytes, block);
+  return one < dev ? Method::ONESHOT : Method::DEVICE;
+}
+
+std::string library_dir() {
+  Dl_info info{};
+  if (dladdr(reinterpret_cast<void *>(&dispatch_init), &info) && info.dli_fname) {
+    std::string p(info.dli_fname);
+    const size_t slash = p.rfind('/');
+    return slash == std::string::npos ? "." : p.substr(0, slash);
+  }
+  return ".";
+}
+
+// the winner among candidates [lo, hi) by predicted time (skipping those
+// `ok` rules out), and whether the ensemble agrees well enough to trust it
+int pick(const float *mean, const float *spread, int lo, int hi, bool *trust,
+         const bool *ok = nullptr) {
+  int best = -1;
+  for (int j = lo; j < hi; ++j)
+    if ((!ok || ok[j - lo]) && (best < 0 || mean[j] < mean[best]))
+      best = j;
+  if (best < 0)
+    best = lo;
+  *trust = spread[best] <= g_spread_limit;
+  return best;
+}
+
+uint64_t config_key(int64_t incount, bool src_host, bool dst_host) {
+  return (uint64_t(incount) << 2) | (src_host ? 2 : 0) | (dst_host ? 1 : 0);
+}
+
+} // namespace
+
+bool eligible(const tempi_desc &d, int64_t incount, int k) {
+  Geometry g;
+  bool empty = false;
+  if (k < 0 || k >= kNumConfigs)
+    return false;
+  if (make_geometry(&d, std::max<int64_t>(incount, 1), 0, 0, 0, &g, &empty) ||
+      empty)
+    return k == 0;
+  const tempi_config &c = kCandidates[k];
+  // the row kernels spread rows, not bytes, over the GPU: they need rows to
+  // fill it
+  const bool many_rows = g.rows >= uint32_t(2 * num_sms());
+  if (c.kernel == 2)
+    return g.block >= 64 && many_rows;
+  if (c.kernel == 3)
+    return g.block >= std::max<int64_t>(16, 4 * c.unroll) && many_rows;
+  return true;
+}
+
+void force_method(int m) { g_forced = m; }
+
+// set while the harness measures: its own packs and sends use the fixed
+// rules (and never re-enter the harness)
+thread_local bool g_measuring = false;
+void set_measuring(bool on) { g_measuring = on; }
+
+void features(const tempi_desc &d, int64_t incount, bool src_host,
+              bool dst_host, float f[TEMPI_MLP_IN]) {
+  Geometry g;
+  bool empty = false;
+  std::memset(f, 0, sizeof(float) * TEMPI_MLP_IN);
+  // pointers are assumed 256-B aligned here; the type's own alignment counts
+  if (make_geometry(&d, std::max<int64_t>(incount, 1), 0, 0, 0, &g, &empty) ||
+      empty)
+    return;
+  int64_t rest = 1;
+  for (uint32_t k = 1; k < g.nd; ++k)
+    rest *= g.cdiv[k].d;
+  const int64_t total = int64_t(g.rows) * g.block;
+  const float s = 1.f / 32.f; // log2 features scaled into [0, ~1]
+  f[0] = float(g.nd) / 5.f;
+  f[1] = lg(g.block) * s;
+  f[2] = g.nd > 0 ? lg(g.cdiv[0].d) * s : 0.f;
+  f[3] = lg(rest) * s;
+  f[4] = g.nd > 0 ? lg(std::abs(double(g.strides[0]))) * s : 0.f;
+  f[5] = g.nd > 1 ? lg(std::abs(double(g.strides[1]))) * s : 0.f;
+  f[6] = lg(total) * s;
+  f[7] = lg(incount) * s;
+  f[8] = lg(g.width) / 4.f;
+  f[9] = src_host ? 1.f : 0.f;
+  f[10] = dst_host ? 1.f : 0.f;
+  f[11] = lg(std::abs(double(d.extent)) * std::max<int64_t>(incount, 1)) * s;
+}
+
+tempi_config choose_config(const tempi_desc &d, int64_t incount) {
+  (void)d;
+  (void)incount;
+  return tempi_config{}; // the fixed rules in launch_geometry
+}
+
+tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
+                           bool dst_host) {
+  const Dispatch mode = env().dispatch;
+  if (mode == Dispatch::HEURISTIC || mode == Dispatch::TABLE || g_measuring)
+    return tempi_config{};
+  const uint64_t key = config_key(incount, src_host, dst_host);
+  {
+    std::lock_guard<std::mutex> l(g_mu);
+    auto it = r.configs.find(key);
+    if (it != r.configs.end()) {
+      counters().dispatch_hit++;
+      return it->second < 0 ? tempi_config{} : kCandidates[it->second];
+    }
+  }
+  counters().dispatch_miss++;
+  int choice = -1;
+  bool trust = false;
+  bool ok[kNumConfigs];
+  for (int k = 0; k < kNumConfigs; ++k)
+    ok[k] = eligible(r.desc, incount, k);
+  if (mode == Dispatch::LEARNED) {
+    float f[TEMPI_MLP_IN], mean[TEMPI_MLP_OUT], spread[TEMPI_MLP_OUT];
+    features(r.desc, incount, src_host, dst_host, f);
+    if (predict(f, mean, spread) == TEMPI_OK)
+      choice = pick(mean, spread, 0, kNumConfigs, &trust, ok);
+  }
+  if (mode == Dispatch::EXHAUSTIVE || (choice >= 0 && !trust)) {
+    float t[kMeasured];
+    if (measure_candidates(r.desc, incount, src_host, dst_host, 1, 2, t) ==
+        TEMPI_OK) {
+      int best = -1;
+      for (int j = 0; j < kNumConfigs; ++j)
+        if (std::isfinite(t[j]) && (best < 0 || t[j] < t[best]))
+          best = j;
+      choice = best;
+    }
+  }
+  std::lock_guard<std::mutex> l(g_mu);
+  r.configs[key] = choice;
+  return choice < 0 ? tempi_config{} : kCandidates[choice];
+}
+
 Method choose_method(TypeRecord &r, int count) {
+  if (g_forced >= 1 && g_forced <= 3)
+    return Method(g_forced);
   switch (env().datatype) {
   case Method::DEVICE:
   case Method::ONESHOT:
@@ -15,23 +385,118 @@ Method choose_method(TypeRecord &r, int count) {
     break;
   }
   const int64_t bytes = int64_t(count) * r.desc.size;
-  auto it = r.methods.find(bytes);
-  if (it != r.methods.end()) {
-    counters().dispatch_hit++;
-    return it->second;
+  {
+    std::lock_guard<std::mutex> l(g_mu);
+    auto it = r.methods.find(bytes);
+    if (it != r.methods.end()) {
+      counters().dispatch_hit++;
+      return it->second;
+    }
   }
   counters().dispatch_miss++;
-  Method m = Method::DEVICE;
+  Method m = Method::DEVICE; // the fixed rule: stay on the GPU
+  const Dispatch mode = env().dispatch;
+  if (mode == Dispatch::TABLE && g_table.loaded) {
+    m = table_method(bytes, r.desc.block);
+  } else if (mode == Dispatch::LEARNED) {
+    float f[TEMPI_MLP_IN], mean[TEMPI_MLP_OUT], spread[TEMPI_MLP_OUT];
+    features(r.desc, count, false, false, f);
+    bool trust = false;
+    if (predict(f, mean, spread) == TEMPI_OK) {
+      const int j = pick(mean, spread, kNumConfigs, kNumConfigs + kNumMethods,
+                         &trust);
+      // an untrusted prediction keeps the fixed rule: timing a transfer
+      // needs a matching receive, which a send cannot arrange by itself
+      if (trust)
+        m = Method(j - kNumConfigs + 1);
+    }
+  }
+  std::lock_guard<std::mutex> l(g_mu);
   r.methods[bytes] = m;
   return m;
 }
 
-tempi_config choose_config(const tempi_desc &d, int64_t incount) {
-  (void)d;
-  (void)incount;
-  return tempi_config{};
+void on_commit(TypeRecord &r) {
+  if (!r.packable || r.desc.size == 0 || env().dispatch != Dispatch::LEARNED ||
+      !g_model.loaded || g_measuring)
+    return;
+  choose_config(r, 1, false, false); // cached for device-to-device packs
 }
 
-void dispatch_init() {}
+void dispatch_init() {
+  const std::string names[] = {env().cache_dir + "/tempi_b200_dispatch.bin",
+                               library_dir() + "/../models/tempi_b200_dispatch.bin"};
+  for (const std::string &n : names)
+    if (load_model_file(n) == TEMPI_OK)
+      break;
+  const std::string tables[] = {env().cache_dir + "/tempi_b200_table.bin",
+                                library_dir() + "/../models/tempi_b200_table.bin"};
+  for (const std::string &n : tables)
+    if (load_table_file(n) == TEMPI_OK)
+      break;
+  if (const char *s = std::getenv("TEMPI_DISPATCH_SPREAD"))
+    g_spread_limit = std::atof(s);
+}
 
 } // namespace tempi
+
+using namespace tempi;
+
+extern "C" int tempi_features(const tempi_desc *d, int64_t incount,
+                              int src_host, int dst_host, float *out) {
+  if (!d || !out)
+    return set_error(TEMPI_ERR_ARG, "null argument");
+  features(*d, incount, src_host != 0, dst_host != 0, out);
+  return TEMPI_OK;
+}
+
+extern "C" int tempi_dispatch_load(const char *model_path,
+                                   const char *table_path) {
+  int err = TEMPI_OK;
+  if (model_path && (err = load_model_file(model_path)))
+    return err ? err : set_error(TEMPI_ERR_ARG, "cannot read %s", model_path);
+  if (table_path && (err = load_table_file(table_path)))
+    return err;
+  return TEMPI_OK;
+}
+
+extern "C" int tempi_dispatch_choose(const tempi_desc *d, int64_t incount,
+                                     int src_host, int dst_host, int mode,
+                                     int *config_index, int *method,
+                                     float *predicted, float *spread) {
+  if (!d)
+    return set_error(TEMPI_ERR_ARG, "null descriptor");
+  int ci = -1, mi = int(Method::DEVICE);
+  float f[TEMPI_MLP_IN], mean[TEMPI_MLP_OUT], sp[TEMPI_MLP_OUT];
+  for (int j = 0; j < TEMPI_MLP_OUT; ++j)
+    mean[j] = sp[j] = NAN;
+  if (mode == 0) { // learned
+    features(*d, incount, src_host != 0, dst_host != 0, f);
+    int err = predict(f, mean, sp);
+    if (err)
+      return err == TEMPI_ERR_UNSUPPORTED
+                 ? set_error(err, "no cost model loaded")
+                 : err;
+    bool trust, ok[kNumConfigs];
+    for (int k = 0; k < kNumConfigs; ++k)
+      ok[k] = eligible(*d, incount, k);
+    ci = pick(mean, sp, 0, kNumConfigs, &trust, ok);
+    mi = pick(mean, sp, kNumConfigs, kNumConfigs + kNumMethods, &trust) -
+         kNumConfigs + 1;
+  } else if (mode == 1) { // restated perf tables
+    if (!g_table.loaded)
+      return set_error(TEMPI_ERR_UNSUPPORTED, "no tables loaded");
+    mi = int(table_method(int64_t(incount) * d->size, d->block));
+  } // mode 2: fixed rules (ci = -1: launch_geometry's choice, DEVICE)
+  if (config_index)
+    *config_index = ci;
+  if (method)
+    *method = mi;
+  for (int j = 0; j < TEMPI_MLP_OUT; ++j) {
+    if (predicted)
+      predicted[j] = mean[j];
+    if (spread)
+      spread[j] = sp[j];
+  }
+  return TEMPI_OK;
+}

@@ -1,18 +1,66 @@
-// Choice of transfer method and kernel configuration for a strided object.
+// Choice of kernel configuration and transfer method for strided objects.
+//
+// The reference picks DEVICE or ONE_SHOT from measured tables (perf.json,
+// src/internal/measure_system.cpp:106-299, cached per (colocated, bytes) in
+// sender.cpp:259-277 and async_operation.cpp:341-368) and picks its kernel
+// word size by a fixed rule.  Here a learned cost model (an FP32 MLP
+// ensemble, mlp.cu) predicts the time of every candidate -- eight kernel
+// configurations and three transfer methods -- from twelve features of the
+// object; the candidate with the smallest predicted time wins.  When the
+// ensemble disagrees about the winner, the candidates are timed for real
+// (exhaustive autotuning).  Choices are cached per type.
 #pragma once
 
 #include "runtime.hpp"
 
 namespace tempi {
 
+constexpr int kNumConfigs = 8; // model outputs 0..7
+constexpr int kNumMethods = 3; // model outputs 8..10: DEVICE, ONE_SHOT, STAGED
+extern const tempi_config kCandidates[kNumConfigs];
+// measured entries: the model's 11 outputs, then the fixed rules' pack +
+// unpack time (the policy without the model)
+constexpr int kFixedRules = TEMPI_MLP_OUT;
+constexpr int kMeasured = TEMPI_MLP_OUT + 1;
+
+// Whether candidate configuration k suits `incount` objects of `d`: a warp
+// per row needs rows of at least 64 B, a shift group of L lanes rows of at
+// least 4L bytes (16 B for L = 4), and both need at least two rows per SM.
+// The harness measures only eligible candidates and the dispatcher chooses
+// only among them.
+bool eligible(const tempi_desc &d, int64_t incount, int k);
+
+// Twelve model inputs for `incount` objects of `d`.
+void features(const tempi_desc &d, int64_t incount, bool src_host,
+              bool dst_host, float out[TEMPI_MLP_IN]);
+
 // Transfer method for `count` objects of a committed type (cached per
 // packed byte count in the record).  TEMPI_DATATYPE_* overrides everything.
 Method choose_method(TypeRecord &r, int count);
 
-// Kernel configuration for one pack/unpack launch.
+// Kernel configuration for one pack/unpack launch of a committed type.
+tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
+                           bool dst_host);
+// ...and for an object with no record (the fixed rules)
 tempi_config choose_config(const tempi_desc &d, int64_t incount);
 
-// Load cached models from TEMPI_CACHE_DIR (called from MPI_Init).
+// Prepare the choice for a newly committed type (MPI_Type_commit).
+void on_commit(TypeRecord &r);
+
+// Load models from TEMPI_CACHE_DIR or next to the library (MPI_Init).
 void dispatch_init();
+
+// Time every candidate: times_us[0..7] = pack + unpack with each kernel
+// configuration, [8..10] = self-send round trip by each method, [11] = pack
+// + unpack by the fixed rules (NaN where not measured).  `what`: bit 0
+// configurations, bit 1 methods.
+int measure_candidates(const tempi_desc &d, int64_t incount, bool src_host,
+                       bool dst_host, int what, int reps, float *times_us);
+
+// Forced method for measurement (-1: none)
+void force_method(int m);
+// While set, kernel configurations come from the fixed rules (the harness
+// measures; it must not recurse into itself).
+void set_measuring(bool on);
 
 } // namespace tempi

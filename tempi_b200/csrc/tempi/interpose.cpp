@@ -80,7 +80,7 @@ int MPI_Type_commit(MPI_Datatype *datatype) {
   int err = libmpi.Type_commit(datatype);
   if (err != MPI_SUCCESS || env().disable || env().no_type_commit)
     return err;
-  commit_type(*datatype);
+  on_commit(*commit_type(*datatype));
   return err;
 }
 
@@ -117,7 +117,7 @@ int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
   if (*position < 0 || *position + bytes > int64_t(outsize))
     return MPI_ERR_TRUNCATE;
   cudaStream_t s = pack_stream();
-  tempi_config cfg = choose_config(r->desc, incount);
+  tempi_config cfg = choose_config(*r, incount, !in.is_device, !out.is_device);
   int e = tempi_pack(&r->desc, in.device_ptr, incount,
                      static_cast<char *>(out.device_ptr) + *position, &cfg, s);
   if (!e) {
@@ -156,7 +156,7 @@ int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
   if (*position < 0 || *position + bytes > int64_t(insize))
     return MPI_ERR_TRUNCATE;
   cudaStream_t s = pack_stream();
-  tempi_config cfg = choose_config(r->desc, outcount);
+  tempi_config cfg = choose_config(*r, outcount, !out.is_device, !in.is_device);
   int e = tempi_unpack(&r->desc,
                        static_cast<const char *>(in.device_ptr) + *position,
                        outcount, out.device_ptr, &cfg, s);

@@ -41,6 +41,9 @@ struct TypeRecord {
   // method chosen per packed byte count (reference SendRecvND's
   // modelChoiceCache_, sender.cpp:259-277)
   std::unordered_map<int64_t, Method> methods;
+  // kernel configuration chosen per (object count, typed-buffer kind,
+  // packed-buffer kind); -1 = the fixed rules
+  std::unordered_map<uint64_t, int> configs;
 };
 
 // Returns nullptr when the type is unknown.  The pointer stays valid until

@@ -57,7 +57,7 @@ int send_strided(TypeRecord &r, Method m, const void *buf, int count, int dest,
                  int tag, MPI_Comm comm) {
   const int64_t bytes = int64_t(count) * r.desc.size;
   cudaStream_t s = pack_stream();
-  tempi_config cfg = choose_config(r.desc, count);
+  tempi_config cfg = choose_config(r, count, false, m == Method::ONESHOT);
   int err = TEMPI_OK;
   switch (m) {
   case Method::ONESHOT: {
@@ -113,7 +113,7 @@ int recv_strided(TypeRecord &r, Method m, void *buf, int count, int source,
                  int tag, MPI_Comm comm, MPI_Status *status) {
   const int64_t bytes = int64_t(count) * r.desc.size;
   cudaStream_t s = pack_stream();
-  tempi_config cfg = choose_config(r.desc, count);
+  tempi_config cfg = choose_config(r, count, false, m == Method::ONESHOT);
   int err = TEMPI_OK;
   switch (m) {
   case Method::ONESHOT: {
@@ -232,7 +232,7 @@ public:
       : m_(m) {
     const int64_t bytes = int64_t(count) * r.desc.size;
     cudaStream_t s = pack_stream();
-    tempi_config cfg = choose_config(r.desc, count);
+    tempi_config cfg = choose_config(r, count, false, m == Method::ONESHOT);
     ev_ = event_acquire();
     void *packed = nullptr;
     int terr = TEMPI_OK;
@@ -349,7 +349,7 @@ public:
       return err;
     const int64_t bytes = int64_t(count_) * r_.desc.size;
     cudaStream_t s = pack_stream();
-    tempi_config cfg = choose_config(r_.desc, count_);
+    tempi_config cfg = choose_config(r_, count_, false, m_ == Method::ONESHOT);
     int terr = TEMPI_OK;
     if (m_ == Method::ONESHOT) {
       terr = tempi_unpack(&r_.desc, host_dev_ptr(host_), count_, buf_, &cfg, s);

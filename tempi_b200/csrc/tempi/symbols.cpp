@@ -75,6 +75,9 @@ bool resolve_symbols() {
     LOAD(Test);
     LOAD(Wait);
     LOAD(Request_free);
+    LOAD(Type_contiguous);
+    LOAD(Type_create_hvector);
+    LOAD(Type_create_resized);
 #undef LOAD
     ok = r;
   });

@@ -41,6 +41,9 @@ struct LibMPI {
   int (*Test)(MPI_Request *, int *, MPI_Status *);
   int (*Wait)(MPI_Request *, MPI_Status *);
   int (*Request_free)(MPI_Request *);
+  int (*Type_contiguous)(int, MPI_Datatype, MPI_Datatype *);
+  int (*Type_create_hvector)(int, int, MPI_Aint, MPI_Datatype, MPI_Datatype *);
+  int (*Type_create_resized)(MPI_Datatype, MPI_Aint, MPI_Aint, MPI_Datatype *);
 };
 
 // Resolve the table once; returns false (and logs) if any symbol is missing.
