@@ -470,6 +470,158 @@ def e2e_bench(torch, sw, mpi, steps, warmup):
             "ms_per_step": round(ms, 3)}
 
 
+def e2e_zero_copy(torch, sw, steps, warmup):
+    """Host-resident data through MPI_Pack/MPI_Unpack with pinned host
+    buffers (device-accessible, so the kernels read and write host memory
+    directly over the link): typed source -> packed (host) -> typed
+    destination (host).  Link bytes counted are the described bytes each
+    kernel reads from or writes to host memory."""
+    from tempi_b200 import _lib
+
+    host = {}
+    for p in sw.pts:
+        key = id(p["src"])
+        if key not in host:
+            hs = torch.empty(p["src"].numel(), dtype=torch.uint8).pin_memory()
+            hs.copy_(p["src"].cpu())
+            host[key] = (hs, torch.empty_like(hs).pin_memory())
+    hp = torch.empty(sw.packed.numel(), dtype=torch.uint8).pin_memory()
+    ops, nbytes = [], 0
+    for p in sw.pts:
+        hs, hd = host[id(p["src"])]
+        n = p["size"] * p["incount"]
+        ops.append(BenchOp(0, p["t"], hs.data_ptr(), hp.data_ptr(), p["incount"], 0, hp.numel(), 0))
+        ops.append(BenchOp(1, p["t"], hd.data_ptr(), hp.data_ptr(), p["incount"], 0, hp.numel(), 0))
+        nbytes += n
+    launches0 = _lib.tempi().tempi_kernel_launches()
+    run_ops(ops, warmup)
+    ms = sum(run_ops(ops, steps)) / steps
+    # at least one pack or unpack kernel per call (the first call per buffer
+    # kind also runs the cost model's inference kernel)
+    assert _lib.tempi().tempi_kernel_launches() - launches0 >= len(ops) * (steps + warmup)
+    return {"value": round(sw.alg_bytes / ms / 1e6, 3), "unit": "GB/s",
+            "h2d_bytes_per_step": int(2 * nbytes), "d2h_bytes_per_step": int(2 * nbytes),
+            "ms_per_step": round(ms, 3),
+            "how": "MPI_Pack/MPI_Unpack on pinned host buffers: kernels read and write "
+                   "host memory directly (link bytes = described bytes)"}
+
+
+def sendrecv_bench(torch, mpi, reps=2):
+    """Config 5: self-sends (MPI_Isend + MPI_Irecv + MPI_Wait x2) of strided
+    device objects by each method, and the method each policy picks."""
+    import time as _t
+
+    from tempi_b200 import _lib
+
+    lib = _lib.tempi()
+    objs = [  # (label, constructor, count)
+        ("2d_byte_b4_4KiB", lambda: mpi.Type_vector(1024, 4, 16, mpi.BYTE), 1),
+        ("2d_byte_b64_1MiB", lambda: mpi.Type_vector(16384, 64, 256, mpi.BYTE), 1),
+        ("3d_float_i4_1MiB", lambda: mpi.Type_create_subarray(
+            [64, 64, 64], [64, 64, 16], [0, 0, 8], mpi.ORDER_C, mpi.FLOAT), 1),
+        ("3d_float_i64_16MiB", lambda: mpi.Type_create_subarray(
+            [256, 256, 256], [256, 256, 64], [0, 0, 67], mpi.ORDER_C, mpi.FLOAT), 1),
+        ("2d_byte_b4096_64MiB", lambda: mpi.Type_vector(16384, 4096, 8192, mpi.BYTE), 1),
+        ("2d_byte_b4096_1GiB", lambda: mpi.Type_vector(262144, 4096, 8192, mpi.BYTE), 1),
+    ]
+    knobs = {"DEVICE": "TEMPI_DATATYPE_DEVICE", "ONE_SHOT": "TEMPI_DATATYPE_ONESHOT",
+             "STAGED": "TEMPI_DATATYPE_STAGED"}
+
+    def set_env(method_var=None, dispatch=None):
+        for v in knobs.values():
+            os.environ.pop(v, None)
+        os.environ.pop("TEMPI_DISPATCH", None)
+        if method_var:
+            os.environ[method_var] = ""
+        if dispatch:
+            os.environ["TEMPI_DISPATCH"] = dispatch
+        lib.tempi_reload_env()
+
+    def round_trip(t, count, src, dst):
+        e1, rr = mpi.Irecv(dst.data_ptr(), count, t, tag=5)
+        e2, rs = mpi.Isend(src.data_ptr(), count, t, tag=5)
+        assert (e1, e2) == (0, 0), _lib.last_error()
+        assert mpi.Wait(rr)[0] == 0 and mpi.Wait(rs)[0] == 0, _lib.last_error()
+
+    rows = []
+    for label, make, count in objs:
+        t0 = make()
+        lbext = mpi.Type_get_extent(t0)[1]
+        src = torch.randint(0, 256, (lbext * count,), dtype=torch.uint8, device="cuda")
+        dst = torch.zeros_like(src)
+        times, chosen = {}, {}
+        for policy, (var, disp) in [("DEVICE", (knobs["DEVICE"], None)),
+                                    ("ONE_SHOT", (knobs["ONE_SHOT"], None)),
+                                    ("STAGED", (knobs["STAGED"], None)),
+                                    ("learned", (None, "learned")),
+                                    ("table", (None, "table")),
+                                    ("fixed", (None, "heuristic"))]:
+            set_env(var, disp)
+            t = make()  # a fresh type per policy: no cached choice carries over
+            assert mpi.Type_commit(t) == 0
+            counts0 = {k: _lib.counter("send_" + k) for k in ("device", "oneshot", "staged")}
+            round_trip(t, count, src, dst)  # warm-up (and the policy's choice)
+            torch.cuda.synchronize()
+            t1 = _t.perf_counter()
+            for _ in range(reps):
+                round_trip(t, count, src, dst)
+            times[policy] = 1e6 * (_t.perf_counter() - t1) / reps
+            after = {k: _lib.counter("send_" + k) for k in ("device", "oneshot", "staged")}
+            chosen[policy] = [k for k in after if after[k] != counts0[k]]
+            mpi.Type_free(t)
+        set_env()
+        best = min(times[m] for m in ("DEVICE", "ONE_SHOT", "STAGED"))
+        rows.append({"object": label, "bytes": int(mpi.Type_size(t0)) * count,
+                     **{k + "_us": round(v, 1) for k, v in times.items()},
+                     "best": min(("DEVICE", "ONE_SHOT", "STAGED"), key=lambda m: times[m]),
+                     "learned_pick": chosen.get("learned"), "table_pick": chosen.get("table"),
+                     "learned_regret": round(times["learned"] / best - 1, 4),
+                     "table_regret": round(times["table"] / best - 1, 4),
+                     "fixed_regret": round(times["fixed"] / best - 1, 4)})
+        del src, dst
+    tot = {p: sum(r[p + "_us"] for r in rows) for p in ("learned", "table", "fixed")}
+    best_tot = sum(min(r[m + "_us"] for m in ("DEVICE", "ONE_SHOT", "STAGED")) for r in rows)
+    return {"objects": rows,
+            "total_regret": {p: round(v / best_tot - 1, 4) for p, v in tot.items()}}
+
+
+def dispatch_sample(torch, n=200, seed=777):
+    """Held-out sample for the learned kernel-configuration choice: fresh
+    random layouts (a seed the model never saw), every eligible candidate
+    timed, the learned pick and the fixed rules against the best."""
+    from tempi_b200 import _lib
+    from tempi_b200 import dispatch_train as DT
+
+    lib = _lib.tempi()
+    rng = np.random.default_rng(seed)
+    times = (ctypes.c_float * 12)()
+    learned, fixed, best = [], [], []
+    t0 = time.time()
+    while len(best) < n and time.time() - t0 < 60:
+        d, incount, th, ph = DT.random_layout(rng)
+        if DT.span_of(d, incount) > (2 << 30) or (th and DT.span_of(d, incount) > (16 << 20)):
+            continue
+        size = d.size * incount
+        reps = 3 if size < (1 << 20) else 2 if size < (64 << 20) else 1
+        _lib.check(lib.tempi_measure(ctypes.byref(d), incount, int(th), int(ph), 1, reps, times))
+        ci = ctypes.c_int(-1)
+        mi = ctypes.c_int(0)
+        if lib.tempi_dispatch_choose(ctypes.byref(d), incount, int(th), int(ph), 0,
+                                     ctypes.byref(ci), ctypes.byref(mi), None, None):
+            return {"error": _lib.last_error()}
+        t = np.frombuffer(times, np.float32)
+        cand = t[:8]
+        best.append(float(np.nanmin(cand)))
+        learned.append(float(cand[ci.value]))
+        fixed.append(float(t[11]))
+    L, F, B = map(np.array, (learned, fixed, best))
+    return {"layouts": len(B), "seed": seed,
+            "learned_total_regret": round(float(L.sum() / B.sum() - 1), 4),
+            "fixed_rules_total_regret": round(float(F.sum() / B.sum() - 1), 4),
+            "learned_within_5pct": round(float(np.mean(L <= 1.05 * B)), 3),
+            "learned_mean_regret": round(float(np.mean(L / B - 1)), 4)}
+
+
 def run_ours(args):
     import torch
 
@@ -529,7 +681,11 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     achieved = top["pack_gbs"]
     halo_res = halo_bench(torch, side) if rank == 0 else None
-    e2e = e2e_bench(torch, sw, mpi, max(1, args.steps // 2), 1)
+    e2e_staged = e2e_bench(torch, sw, mpi, max(1, args.steps // 2), 1)
+    e2e_zc = e2e_zero_copy(torch, sw, max(1, args.steps // 2), 1)
+    e2e = dict(e2e_zc, staged=e2e_staged)
+    send_res = sendrecv_bench(torch, mpi) if rank == 0 and not args.no_sendrecv else None
+    disp_res = dispatch_sample(torch) if rank == 0 and not args.no_sendrecv else None
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
@@ -546,6 +702,8 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "e2e": e2e,
         "halo": halo_res,
+        "sendrecv": send_res,
+        "dispatch": disp_res,
         "sweep": [{"p": r["label"], "k": r["kernel"], "pack_gbs": round(r["pack_gbs"], 1),
                    "unpack_gbs": round(r["unpack_gbs"], 1)} for r in table],
     }
@@ -601,6 +759,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sendrecv", action="store_true",
+                    help="skip the self-send and dispatch-regret sections")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the sweep only (for launch-list captures)")
     ap.add_argument("--profile-point", default=None,

@@ -236,6 +236,9 @@ public:
     ev_ = event_acquire();
     void *packed = nullptr;
     int terr = TEMPI_OK;
+    (m == Method::ONESHOT  ? counters().send_oneshot
+     : m == Method::STAGED ? counters().send_staged
+                           : counters().send_device)++;
     if (m == Method::ONESHOT) {
       host_ = slab_alloc(Space::HOST_MAPPED, bytes);
       packed = host_;

@@ -1,0 +1,90 @@
+"""The learned dispatch with the committed model (tempi_b200/models/):
+the harness measures every eligible candidate, the dispatcher picks among
+them, MPI_Pack uses the pick and stays bit-exact, and on fresh layouts the
+model's picks cost less in total than the fixed rules' (what the network
+gains over the method without it)."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle import types as T
+from tempi_b200 import _lib, dispatch_train as DT, mpi
+
+from . import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+MODEL = os.path.join(DT.MODELS, DT.MODEL_FILE)
+TABLE = os.path.join(DT.MODELS, DT.TABLE_FILE)
+
+
+@pytest.fixture(scope="module")
+def model(cuda, mpi_init):
+    assert os.path.exists(MODEL), "the trained cost model is missing"
+    _lib.check(_lib.tempi().tempi_dispatch_load(MODEL.encode(), TABLE.encode()))
+
+
+def test_measure_covers_eligible_candidates(model):
+    lib = _lib.tempi()
+    t = (ctypes.c_float * 12)()
+    d = _lib.Desc.make(4, 1 << 22, 1000, [2000], [2048])
+    _lib.check(lib.tempi_measure(ctypes.byref(d), 1, 0, 0, 3, 2, t))
+    v = np.frombuffer(t, np.float32)
+    assert np.isfinite(v).all() and (v > 0).all(), v  # 1000-B rows: all eligible
+    d = _lib.Desc.make(0, 1 << 20, 1 << 20, [], [])  # one contiguous block
+    _lib.check(lib.tempi_measure(ctypes.byref(d), 1, 0, 0, 1, 2, t))
+    v = np.frombuffer(t, np.float32)
+    assert np.isfinite(v[:3]).all() and np.isnan(v[3:8]).all() and np.isfinite(v[11])
+
+
+def test_choice_is_eligible_and_pack_stays_exact(model):
+    rng = np.random.default_rng(11)
+    before = _lib.counter("dispatch_miss")
+    for _ in range(20):
+        ty = H.random_type(rng).commit()  # MPI_Type_commit runs the model
+        err, d = mpi.describe(ty.h)
+        if err:
+            continue
+        ci, mi = ctypes.c_int(-2), ctypes.c_int(0)
+        pred = (ctypes.c_float * 11)()
+        _lib.check(_lib.tempi().tempi_dispatch_choose(ctypes.byref(d), 2, 0, 0, 0,
+                                                       ctypes.byref(ci), ctypes.byref(mi),
+                                                       pred, None))
+        assert 0 <= ci.value < 8 and 1 <= mi.value <= 3
+        assert np.isfinite(np.frombuffer(pred, np.float32)).all()
+        import torch
+
+        src_np = H.splitmix_bytes(max(ty.o.extent * 2, 1) + 64, 3)
+        src = torch.from_numpy(src_np).cuda()
+        out = torch.zeros(max(ty.o.size * 2, 1), dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        e, pos = mpi.Pack(src.data_ptr(), 2, ty.h, out.data_ptr(), out.numel())
+        assert e == 0
+        assert out.cpu().numpy()[:pos].tobytes() == T.pack(ty.o, src_np, 2).tobytes()
+    assert _lib.counter("dispatch_miss") > before
+
+
+def test_learned_beats_fixed_rules_on_fresh_layouts(model):
+    lib = _lib.tempi()
+    rng = np.random.default_rng(4242)  # layouts the model never saw
+    t = (ctypes.c_float * 12)()
+    L, F, B = [], [], []
+    while len(B) < 120:
+        d, incount, th, ph = DT.random_layout(rng)
+        if DT.span_of(d, incount) > (1 << 30) or th or ph:
+            continue
+        _lib.check(lib.tempi_measure(ctypes.byref(d), incount, 0, 0, 1, 2, t))
+        ci, mi = ctypes.c_int(-1), ctypes.c_int(0)
+        _lib.check(lib.tempi_dispatch_choose(ctypes.byref(d), incount, 0, 0, 0,
+                                              ctypes.byref(ci), ctypes.byref(mi), None, None))
+        v = np.frombuffer(t, np.float32)
+        B.append(np.nanmin(v[:8]))
+        L.append(v[ci.value])
+        F.append(v[11])
+    L, F, B = map(np.array, (L, F, B))
+    learned, fixed = L.sum() / B.sum() - 1, F.sum() / B.sum() - 1
+    print(f"total-time regret: learned {learned:.3f}, fixed rules {fixed:.3f}")
+    assert learned < fixed
+    assert learned < 0.10
