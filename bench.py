@@ -16,9 +16,19 @@ Also reported on the same GPU in the same run:
   halo       26-region halo of a 256^3 grid of doubles (radius 2): 26 plain
              MPI_Pack calls vs one batched launch vs one CUDA-graph replay,
              plus the mixed batch of 8 grids
-  e2e        the same sweep with host-resident data: each step copies every
-             source object span host->device, packs, copies the packed bytes
-             back, then the reverse for the unpack
+  e2e        the same sweep with host-resident data through MPI_Pack /
+             MPI_Unpack on pinned host buffers (the kernels read and write
+             host memory over the link); `e2e.staged` is the alternative that
+             copies every source span host->device, packs, copies the packed
+             bytes back, and the reverse for the unpack
+  sendrecv   config 5: self-sends of strided device objects (4 KiB - 1 GiB)
+             by DEVICE, ONE_SHOT and STAGED, and what the learned model, the
+             restated perf-table model and the fixed rules pick
+  dispatch   a held-out sample (seed never trained on) of random layouts:
+             total-time regret of the learned kernel-configuration choice
+             and of the fixed rules against exhaustive measurement
+  config1    config 1 (vector 1024 x 64 B, stride 512) through the interposer
+             on host buffers (the library's host pack) and on device buffers
   cpu_baseline  the oracle's C type-map walker (a port of what the underlying
              MPI's host MPI_Pack does) on one host core, on a bounded sample
 
@@ -622,6 +632,55 @@ def dispatch_sample(torch, n=200, seed=777):
             "learned_mean_regret": round(float(np.mean(L / B - 1)), 4)}
 
 
+def config1_bench(torch, mpi, reps=200):
+    """Config 1: MPI_Type_vector(1024, 64, 512, MPI_BYTE), incount 1, 512 KiB
+    of seeded random bytes.  With host buffers the interposed MPI_Pack hands
+    the call to the underlying library (its host pack, as the reference does,
+    src/pack.cpp:51-55); the same type on device buffers runs the kernel.
+    Both are checked byte for byte against each other and timed per call."""
+    t = mpi.Type_vector(1024, 64, 512, mpi.BYTE)
+    assert mpi.Type_commit(t) == 0
+    src = np.random.default_rng(0).integers(0, 256, 512 * 1024, dtype=np.uint8)
+    out = np.zeros(65536, np.uint8)
+    back = np.full_like(src, 0xAA)
+    dsrc = torch.from_numpy(src).cuda()
+    dout = torch.zeros(65536, dtype=torch.uint8, device="cuda")
+    dback = torch.full_like(dsrc, 0xAA)
+    torch.cuda.synchronize()
+
+    def run(a, b, c):
+        e1, _ = mpi.Pack(a, 1, t, b, 65536)
+        e2, _ = mpi.Unpack(b, 65536, c, 1, t)
+        assert (e1, e2) == (0, 0)
+
+    res = {}
+    for name, (a, b, c) in (("host_library", (src.ctypes.data, out.ctypes.data, back.ctypes.data)),
+                            ("device_kernel", (dsrc.data_ptr(), dout.data_ptr(), dback.data_ptr()))):
+        run(a, b, c)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            run(a, b, c)
+        us = 1e6 * (time.perf_counter() - t0) / reps
+        res[name] = {"pack_plus_unpack_us": round(us, 2),
+                     "gbs": round(2 * 2 * 65536 / us / 1e3, 3)}
+    same = out.tobytes() == dout.cpu().numpy().tobytes()
+    gaps = bool((back.reshape(1024, 512)[:1023, 64:] == 0xAA).all())
+    mpi.Type_free(t)
+    return dict(res, packed_bytes=65536, host_equals_device=same, gaps_untouched=gaps,
+                timing="host wall clock per MPI_Pack+MPI_Unpack pair, 200 pairs")
+
+
+def reduce_max(value, dist, device=None):
+    """Max over ranks of a per-rank time (replicas: one process per GPU)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args):
     import torch
 
@@ -661,11 +720,7 @@ def run_ours(args):
     if launches < len(ops) * args.steps:
         raise RuntimeError(f"only {launches} TEMPI kernel launches in the timed region: "
                            "the MPI calls did not reach the interposer's GPU path")
-    ms = sum(times) / len(times)
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(sum(times) / len(times), dist, dev)
     value = world * sw.alg_bytes / ms / 1e6  # GB/s over all replicas
 
     if args.no_extras:
@@ -685,6 +740,7 @@ def run_ours(args):
     e2e_zc = e2e_zero_copy(torch, sw, max(1, args.steps // 2), 1)
     e2e = dict(e2e_zc, staged=e2e_staged)
     send_res = sendrecv_bench(torch, mpi) if rank == 0 and not args.no_sendrecv else None
+    c1_res = config1_bench(torch, mpi) if rank == 0 else None
     disp_res = dispatch_sample(torch) if rank == 0 and not args.no_sendrecv else None
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
@@ -702,6 +758,7 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "e2e": e2e,
         "halo": halo_res,
+        "config1": c1_res,
         "sendrecv": send_res,
         "dispatch": disp_res,
         "sweep": [{"p": r["label"], "k": r["kernel"], "pack_gbs": round(r["pack_gbs"], 1),
