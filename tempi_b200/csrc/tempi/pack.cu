@@ -69,44 +69,40 @@ __global__ void __launch_bounds__(512)
   constexpr int U = kUnroll;
   const uint32_t nthreads = gridDim.x * blockDim.x;
   const uint32_t total = g.total_words;
-  uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-
-  for (; w + (U - 1) * nthreads < total; w += U * nthreads) {
+  // every pass keeps U independent loads in flight; the last pass is
+  // predicated instead of falling back to one load at a time
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < total;
+       w += U * nthreads) {
     int64_t so[U];
+    bool in[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const uint32_t ww = w + u * nthreads;
-      const uint32_t row = fastdiv(ww, g.wdiv);
-      const uint32_t col = ww - row * g.wpr;
+      in[u] = ww < total;
+      const uint32_t row = fastdiv(in[u] ? ww : 0, g.wdiv);
+      const uint32_t col = (in[u] ? ww : 0) - row * g.wpr;
       so[u] = row_offset<ND>(row, g) + int64_t(col) * W;
     }
     T v[U];
     if (!UNPACK) {
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        v[u] = __ldg(reinterpret_cast<const T *>(strided + so[u]));
+        if (in[u])
+          v[u] = __ldg(reinterpret_cast<const T *>(strided + so[u]));
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        reinterpret_cast<T *>(packed)[w + u * nthreads] = v[u];
+        if (in[u])
+          reinterpret_cast<T *>(packed)[w + u * nthreads] = v[u];
     } else {
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        v[u] = __ldg(reinterpret_cast<const T *>(packed) + (w + u * nthreads));
+        if (in[u])
+          v[u] = __ldg(reinterpret_cast<const T *>(packed) + (w + u * nthreads));
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        *reinterpret_cast<T *>(strided + so[u]) = v[u];
+        if (in[u])
+          *reinterpret_cast<T *>(strided + so[u]) = v[u];
     }
-  }
-  for (; w < total; w += nthreads) {
-    const uint32_t row = fastdiv(w, g.wdiv);
-    const uint32_t col = w - row * g.wpr;
-    const int64_t so = row_offset<ND>(row, g) + int64_t(col) * W;
-    if (!UNPACK)
-      reinterpret_cast<T *>(packed)[w] =
-          __ldg(reinterpret_cast<const T *>(strided + so));
-    else
-      *reinterpret_cast<T *>(strided + so) =
-          __ldg(reinterpret_cast<const T *>(packed) + w);
   }
 }
 
@@ -125,18 +121,18 @@ __global__ void __launch_bounds__(512)
     T *p = reinterpret_cast<T *>(packed + int64_t(row) * g.block);
     const T *src = UNPACK ? p : s;
     T *dst = UNPACK ? s : p;
-    uint32_t c = lane;
-    for (; c + 32 * (U - 1) < wpr; c += 32 * U) {
+    // U predicated loads in flight per lane, whatever the row length
+    for (uint32_t c = lane; c < wpr; c += 32 * U) {
       T v[U];
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        v[u] = __ldg(src + c + 32 * u);
+        if (c + 32 * u < wpr)
+          v[u] = __ldg(src + c + 32 * u);
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        dst[c + 32 * u] = v[u];
+        if (c + 32 * u < wpr)
+          dst[c + 32 * u] = v[u];
     }
-    for (; c < wpr; c += 32)
-      dst[c] = __ldg(src + c);
   }
 }
 
