@@ -102,27 +102,49 @@ __device__ __forceinline__ void copy_chunk(const BatchRegion &r, uint32_t w0,
   }
 }
 
-__global__ void __launch_bounds__(kBatchThreads)
+// Index of the last region whose first chunk is <= chunk, found by warp 0:
+// each round the lanes sample 32 evenly spaced entries of the remaining
+// stretch with one coalesced load and a ballot narrows it 32-fold, so n
+// regions take ceil(log32 n) dependent loads (one for a 26-region halo, two
+// for up to 1024 regions) instead of a binary search's log2 n.
+__device__ __forceinline__ int find_region(const BatchRegion *__restrict__ r,
+                                           int n, uint32_t chunk,
+                                           uint32_t lane) {
+  int base = 0, len = n;
+  while (true) {
+    const int step = (len + 31) / 32;
+    const int off = int(lane) * step;
+    const bool le = off < len && r[base + off].chunk_begin <= chunk;
+    const unsigned m = __ballot_sync(0xffffffffu, le);
+    const int seg = 31 - __clz(m); // the stretch's first entry always qualifies
+    base += seg * step;
+    if (step == 1)
+      return base;
+    len = min(step, len - seg * step);
+  }
+}
+
+__global__ void __launch_bounds__(kBatchThreads, 3)
     k_batch(const BatchRegion *__restrict__ regions, int nregions,
             uint32_t total_chunks, int unpack) {
   __shared__ BatchRegion sr;
   __shared__ int cur;
+  const uint32_t lane = threadIdx.x & 31;
   if (threadIdx.x == 0)
     cur = -1;
   __syncthreads();
   for (uint32_t chunk = blockIdx.x; chunk < total_chunks; chunk += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int lo = 0, hi = nregions - 1; // last region with chunk_begin <= chunk
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (regions[mid].chunk_begin <= chunk)
-          lo = mid;
-        else
-          hi = mid - 1;
-      }
-      if (lo != cur) {
-        sr = regions[lo];
-        cur = lo;
+    if (threadIdx.x < 32) {
+      const int idx = find_region(regions, nregions, chunk, lane);
+      if (idx != cur) { // the warp copies the record, a word per lane
+        constexpr int kWords = sizeof(BatchRegion) / 4;
+        const uint32_t *from = reinterpret_cast<const uint32_t *>(regions + idx);
+        uint32_t *to = reinterpret_cast<uint32_t *>(&sr);
+        for (int w = lane; w < kWords; w += 32)
+          to[w] = from[w];
+        __syncwarp();
+        if (lane == 0)
+          cur = idx;
       }
     }
     __syncthreads();
@@ -288,7 +310,8 @@ extern "C" int tempi_batch_replay(tempi_batch *b, void *stream) {
 constexpr int kStaticBatchRegions = 1024;
 constexpr int kMaxDevices = 64;
 
-static_assert(sizeof(BatchRegion) == 168, "table entry size is documented");
+static_assert(sizeof(BatchRegion) == 168 && sizeof(BatchRegion) % 4 == 0,
+              "table entry size is documented");
 static __device__ __align__(256) BatchRegion g_static_regions[kStaticBatchRegions];
 
 static std::mutex g_static_mu;

@@ -134,3 +134,44 @@ def test_batch_counts_one_launch(cuda, mpi_init):
     halo.pack_plain(g, data.data_ptr(), packed.data_ptr())
     assert _lib.tempi().tempi_kernel_launches() == n0 + 26
     b.close()
+
+
+def test_batch_of_1500_regions(cuda, mpi_init):
+    """More regions than one warp-search round can cover twice (three rounds
+    of the region lookup), each a small strided object of its own."""
+    import torch
+
+    rng = np.random.default_rng(9)
+    n = 1500
+    buf_np = H.splitmix_bytes(n * 256, 77)
+    buf = torch.from_numpy(buf_np).cuda()
+    regs, wants, offs, pos = [], [], [], 0
+    for i in range(n):
+        bl = int(rng.integers(1, 9))
+        cnt = int(rng.integers(1, 6))
+        st = bl + int(rng.integers(0, 8))
+        d = _lib.Desc.make(0, st * cnt, bl, [cnt], [st])
+        base = i * 256
+        o = T.hvector(cnt, 1, st, T.contiguous(bl, T.BYTE))
+        wants.append(T.pack(o, buf_np, 1, origin=base))
+        offs.append(pos)
+        pos += d.size
+        regs.append((base, d))
+    packed = torch.zeros(pos, dtype=torch.uint8, device="cuda")
+    rr = []
+    for (base, d), off in zip(regs, offs):
+        r = _lib.Region()
+        r.origin = buf.data_ptr() + base
+        r.packed = packed.data_ptr() + off
+        r.desc = d
+        r.incount = 1
+        rr.append(r)
+    import ctypes
+
+    arr = (_lib.Region * n)(*rr)
+    h = ctypes.c_void_p()
+    _lib.check(_lib.tempi().tempi_batch_create(arr, n, 0, ctypes.byref(h)))
+    _lib.check(_lib.tempi().tempi_batch_launch(h, None))
+    torch.cuda.synchronize()
+    assert packed.cpu().numpy().tobytes() == np.concatenate(wants).tobytes()
+    _lib.tempi().tempi_batch_destroy(h)
