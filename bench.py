@@ -72,6 +72,19 @@ def sweep_points(seed=2026):
     return pts
 
 
+def traffic_from_profiles(label, direction="pack"):
+    """Per-launch DRAM bytes of a sweep point's kernel from the committed ncu
+    summary (profiles/traffic.txt), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = line.split()
+        if len(f) == 3 and not line.startswith("#") and f[0] == label and f[1] == direction:
+            return int(f[2])
+    return None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -751,7 +764,9 @@ def run_ours(args):
             "bound": "hbm", "kernel": f"{top['label']} pack ({top['kernel']})",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-            "traffic": None, "share_of_kernel_time": round(top["pack_ms"] / total_t, 3),
+            "traffic": traffic_from_profiles(top["label"]),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/traffic.txt",
+            "share_of_kernel_time": round(top["pack_ms"] / total_t, 3),
             "alg_bytes_per_launch": 2 * top["packed_bytes"],
         },
         "clocks": clk.summary(),

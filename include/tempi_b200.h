@@ -204,6 +204,12 @@ int tempi_dispatch_choose(const tempi_desc *d, int64_t incount,
                           int *config_index, int *method, float *predicted,
                           float *spread);
 
+/* The table model's interpolation (reference measure_system.cpp:181-299):
+   cols <= 0: a 1-D table, entry i = 2^i bytes; otherwise rows x cols, entry
+   [i][j] = 2^(2i+6) bytes packed from blocks of 2^j bytes. */
+double tempi_table_interp(const double *table, int rows, int cols,
+                          int64_t bytes, int64_t block);
+
 /* ---- runtime ------------------------------------------------------------ */
 /* TEMPI's internal non-blocking stream (a cudaStream_t) on which the MPI
    entry points launch (reference kernStream, src/internal/streams.cpp:16-28).

@@ -500,3 +500,16 @@ extern "C" int tempi_dispatch_choose(const tempi_desc *d, int64_t incount,
   }
   return TEMPI_OK;
 }
+
+extern "C" double tempi_table_interp(const double *table, int rows, int cols,
+                                     int64_t bytes, int64_t block) {
+  using namespace tempi;
+  if (!table || rows <= 0)
+    return NAN;
+  if (cols <= 0)
+    return table_1d(std::vector<double>(table, table + rows), bytes);
+  std::vector<std::vector<double>> a(rows);
+  for (int i = 0; i < rows; ++i)
+    a[i].assign(table + size_t(i) * cols, table + size_t(i + 1) * cols);
+  return table_2d(a, bytes, block);
+}
