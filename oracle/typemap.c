@@ -117,21 +117,25 @@ static void walk(walker *w, int64_t n, int64_t base) {
 
 typedef struct {
   walker w;
-  int64_t root, obj0, obj1; /* objects [obj0, obj1) */
-  int64_t j0, j1;           /* or, with one object, root blocks [j0, j1) */
-  int64_t extent;
+  int64_t node;   /* the node whose blocks are the work units */
+  int64_t off;    /* byte offset of `node` inside one object */
+  int64_t extent; /* extent of one object */
+  int64_t per;    /* units per object (blocks of `node`, or 1) */
+  int64_t u0, u1; /* this job's units [u0, u1) */
 } job;
 
 static void *run_job(void *p) {
   job *jb = (job *)p;
   walker *w = &jb->w;
-  if (jb->j1 > jb->j0) {
-    const onode *t = &w->nodes[jb->root];
-    for (int64_t j = jb->j0; j < jb->j1; ++j)
-      walk_run(w, t->child, j * t->stride, t->bl, w->nodes[t->child].extent);
-  } else {
-    for (int64_t i = jb->obj0; i < jb->obj1; ++i)
-      walk(w, jb->root, i * jb->extent);
+  const onode *t = &w->nodes[jb->node];
+  for (int64_t u = jb->u0; u < jb->u1; ++u) {
+    const int64_t i = u / jb->per, j = u % jb->per;
+    const int64_t base = i * jb->extent + jb->off;
+    if (jb->per > 1)
+      walk_run(w, t->child, base + j * t->stride, t->bl,
+               w->nodes[t->child].extent);
+    else
+      walk(w, jb->node, base);
   }
   flush(w);
   return 0;
@@ -139,8 +143,14 @@ static void *run_job(void *p) {
 
 /* Pack (unpack=0) or unpack (unpack=1) `incount` objects of node `root`.
    `typed` is the typed buffer, `packed` the contiguous one.  Returns the
-   number of packed bytes.  With nthreads > 1 the objects (or, for a single
-   HVEC object, its blocks) are split evenly across POSIX threads. */
+   number of packed bytes.
+
+   With nthreads > 1 the work is split into units that each own one
+   contiguous range of the packed buffer: the blocks of the outermost strided
+   vector, found by stepping through one-block wrappers (a subarray's start
+   displacement, a resized bound, a count-1 vector), times the objects.
+   Each POSIX thread takes an even share of the units.  Without such a
+   vector the units are whole objects. */
 int64_t oracle_walk(const onode *nodes, int64_t root, const int64_t *bls,
                     const int64_t *displs, const int64_t *kids, char *typed,
                     int64_t incount, char *packed, int unpack, int nthreads) {
@@ -152,16 +162,34 @@ int64_t oracle_walk(const onode *nodes, int64_t root, const int64_t *bls,
     nthreads = 1;
   if (nthreads > 256)
     nthreads = 256;
-  job jobs[256];
-  int64_t parts = 1, by_blocks = 0;
-  if (nthreads > 1 && incount >= nthreads) {
-    parts = nthreads;
-  } else if (nthreads > 1 && incount == 1 && t->kind == O_HVEC && !t->dense &&
-             t->count >= nthreads) {
-    parts = nthreads;
-    by_blocks = 1;
+
+  int64_t node = root, off = 0, per = 1;
+  for (;;) {
+    const onode *n = &nodes[node];
+    if (n->dense)
+      break;
+    if (n->kind == O_HIND && n->count == 1 && bls[n->aux] == 1) {
+      off += displs[n->aux];
+      node = n->child;
+    } else if (n->kind == O_HVEC && n->count == 1 && n->bl == 1) {
+      node = n->child;
+    } else {
+      break;
+    }
   }
-  const int64_t per_block = t->bl * nodes[t->child].size;
+  const onode *s = &nodes[node];
+  if (!s->dense && s->kind == O_HVEC && s->count > 1 &&
+      s->count * s->bl * nodes[s->child].size == t->size)
+    per = s->count;
+  else {
+    node = root;
+    off = 0;
+  }
+  const int64_t units = incount * per;
+  const int64_t unit_bytes = t->size / per;
+  int64_t parts = nthreads < units ? nthreads : units;
+
+  job jobs[256];
   for (int64_t p = 0; p < parts; ++p) {
     job *jb = &jobs[p];
     memset(jb, 0, sizeof(*jb));
@@ -172,17 +200,13 @@ int64_t oracle_walk(const onode *nodes, int64_t root, const int64_t *bls,
     jb->w.in = typed;
     jb->w.out = packed;
     jb->w.unpack = unpack;
-    jb->root = root;
+    jb->node = node;
+    jb->off = off;
     jb->extent = t->extent;
-    if (by_blocks) {
-      jb->j0 = t->count * p / parts;
-      jb->j1 = t->count * (p + 1) / parts;
-      jb->w.pos = jb->j0 * per_block;
-    } else {
-      jb->obj0 = incount * p / parts;
-      jb->obj1 = incount * (p + 1) / parts;
-      jb->w.pos = jb->obj0 * t->size;
-    }
+    jb->per = per;
+    jb->u0 = units * p / parts;
+    jb->u1 = units * (p + 1) / parts;
+    jb->w.pos = jb->u0 * unit_bytes;
   }
   if (parts == 1) {
     run_job(&jobs[0]);

@@ -23,7 +23,7 @@ equivalent:
    tempi_b200/models/) and a JSON report.
 
     python -m tempi_b200.dispatch_train --types 50000 --heldout 5000 \\
-        --budget-s 900 --out gpurun_out/dispatch
+        --budget-s 900 --out /tmp/dispatch
 """
 from __future__ import annotations
 

@@ -134,6 +134,32 @@ def test_c_walker_threads_match(mpi_init):
     assert single.tobytes() == one[: o.size].tobytes()
 
 
+def test_c_walker_thread_split_through_wrappers():
+    """Threaded walks split a subarray (start displacement wrapper), a
+    resized type and a count-1 vector wrapper at their inner vector's
+    blocks; every split must write what one thread writes, for pack and
+    unpack, with one object and with several."""
+    sub = T.subarray([64, 48, 40], [30, 20, 16], [5, 7, 9], T.ORDER_C, T.named(4))
+    res = T.resized(T.vector(37, 3, 5, T.named(2)), -8, 500)
+    wrap = T.hvector(1, 1, 0, T.vector(50, 7, 9, T.BYTE))
+    fort = T.subarray([33, 12], [20, 5], [3, 4], T.ORDER_FORTRAN, T.named(8))
+    for o in (sub, res, wrap, fort):
+        w = W.Walker(o)
+        for cnt in (1, 3):
+            lo = min(0, o.true_lb)
+            hi = o.true_ub + (cnt - 1) * o.extent
+            buf = H.splitmix_bytes(hi - lo + 16, cnt)
+            one = w.pack(buf, cnt, origin=-lo, nthreads=1)
+            assert one.tobytes() == T.pack(o, buf, cnt, origin=-lo).tobytes()
+            for nt in (2, 7, 64):
+                assert w.pack(buf, cnt, origin=-lo, nthreads=nt).tobytes() == one.tobytes()
+                a = np.zeros_like(buf)
+                b = np.zeros_like(buf)
+                w.unpack(one, a, cnt, origin=-lo, nthreads=1)
+                w.unpack(one, b, cnt, origin=-lo, nthreads=nt)
+                assert a.tobytes() == b.tobytes()
+
+
 def test_random_types_numpy_vs_c_walker():
     rng = np.random.default_rng(5)
     for _ in range(200):

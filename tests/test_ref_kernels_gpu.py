@@ -7,8 +7,8 @@ every stride and the base pointer, which it does not check), the reference
 packers, TEMPI's kernels and the type-map oracle write the same bytes.
 
 Timing: both kernels on the same buffers, CUDA events on one stream; the
-table is printed and written to gpurun_out/ref_vs_tempi.json when that
-directory exists (the summary lives in profiles/).
+table is printed, and written to $TEMPI_RESULTS_DIR/ref_vs_tempi.json when
+that variable names a directory.
 """
 import ctypes
 import json
@@ -143,8 +143,8 @@ def test_reference_kernels_match_tempi_and_oracle(cuda, mpi_init, ref):
             "unpack_speedup": round(times[("reference", 1)] / times[("tempi", 1)], 2),
         })
     print(json.dumps(results, indent=1))
-    out = os.path.join(ROOT, "gpurun_out")
-    if os.path.isdir(out):
+    out = os.environ.get("TEMPI_RESULTS_DIR", "")
+    if out and os.path.isdir(out):
         with open(os.path.join(out, "ref_vs_tempi.json"), "w") as f:
             json.dump(results, f, indent=1)
 
