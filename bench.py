@@ -204,7 +204,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    nthreads = os.cpu_count() or 1
+    nthreads = len(os.sched_getaffinity(0)) or 1
     items = _oracle_points(sweep_points())
     bufs = cpu_buffers(items)
     for _ in range(args.warmup):

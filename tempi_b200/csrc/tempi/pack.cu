@@ -137,16 +137,19 @@ __global__ void __launch_bounds__(512)
 }
 
 // Row copy for rows whose source and destination disagree modulo 16.
-// Each group of L lanes owns one row and each lane K consecutive 16-B
-// destination words per pass, so K independent loads are in flight per lane.
-// Destination bytes are written as 16-B aligned words (head and tail bytes
-// singly); the source is read as the 16-B aligned words that cover it, and
-// each destination word is assembled from two neighbouring source words with
-// funnel shifts.  The word after a lane's last one is the next lane's first,
-// passed with a shuffle, so every source byte is loaded once.  Aligned 16-B
-// reads that stick out past either end of a row stay inside a 16-B chunk that
-// holds a row byte, so they never leave the row's memory page; their extra
-// bytes are discarded.
+// The destination row is covered by nw 16-B aligned words, the first and the
+// last possibly partial.  Each group of L lanes owns one row and each lane K
+// of its words per pass (lane l: words base + l + k*L), so K independent
+// loads are in flight per lane and every instruction of a group touches L
+// consecutive words: behind the L2 the order would not matter, but reads of
+// host memory over the link are issued per instruction, and wide contiguous
+// requests are what the link moves efficiently.  Word j is assembled with
+// funnel shifts from the 16-B aligned source words j and j+1 that cover it;
+// word j+1 comes from the next lane by shuffle, so every source word is
+// loaded once.  A source word is loaded only if it holds a byte of the row,
+// so no access leaves the 16-B chunks the row touches.  Whole words are
+// stored as one 16-B store; the partial end words as aligned 8/4/2/1-byte
+// pieces of exactly the row's bytes.
 constexpr int kShiftWords = 4;
 
 __device__ __forceinline__ uint4 realign(const uint4 &a, const uint4 &b,
@@ -162,60 +165,86 @@ __device__ __forceinline__ uint4 realign(const uint4 &a, const uint4 &b,
                     __funnelshift_r(x2, x3, sh), __funnelshift_r(x3, x4, sh));
 }
 
+__device__ __forceinline__ uint32_t word32(const uint4 &v, uint32_t i) {
+  return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
+}
+
+// bytes [a, b) of v to w + a (w 16-B aligned), in the widest aligned pieces
+__device__ __forceinline__ void store_part(char *w, const uint4 &v, uint32_t a,
+                                           uint32_t b) {
+  while (a < b) {
+    const uint32_t x = word32(v, a >> 2);
+    if ((a & 7) == 0 && a + 8 <= b) {
+      *reinterpret_cast<uint2 *>(w + a) = make_uint2(x, word32(v, (a >> 2) + 1));
+      a += 8;
+    } else if ((a & 3) == 0 && a + 4 <= b) {
+      *reinterpret_cast<uint32_t *>(w + a) = x;
+      a += 4;
+    } else if ((a & 1) == 0 && a + 2 <= b) {
+      *reinterpret_cast<uint16_t *>(w + a) = uint16_t(x >> ((a & 3) * 8));
+      a += 2;
+    } else {
+      w[a] = char(x >> ((a & 3) * 8));
+      a += 1;
+    }
+  }
+}
+
 template <int L>
 __device__ __forceinline__ void shifted_row(const char *__restrict__ s,
                                             char *__restrict__ d, uint32_t n,
                                             uint32_t lane) {
   constexpr int K = kShiftWords;
-  const uint32_t head =
-      min(n, uint32_t((16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15));
-  for (uint32_t i = lane; i < head; i += L)
-    d[i] = s[i];
-  const uint32_t nb = (n - head) >> 4; // whole destination words
-  const uint32_t tail0 = head + (nb << 4);
-  for (uint32_t i = tail0 + lane; i < n; i += L)
-    d[i] = s[i];
-  if (nb == 0)
-    return;
-  const char *sa = s + head;
-  uint4 *dw = reinterpret_cast<uint4 *>(d + head);
-  const uint32_t o = reinterpret_cast<uintptr_t>(sa) & 15;
-  const uint4 *aw = reinterpret_cast<const uint4 *>(sa - o);
-  if (o == 0) {
-    for (uint32_t base = 0; base < nb; base += L * K) {
-      const uint32_t j0 = base + lane * K;
-      uint4 v[K];
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-        if (j0 + k < nb)
-          v[k] = __ldg(aw + j0 + k);
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-        if (j0 + k < nb)
-          dw[j0 + k] = v[k];
-    }
-    return;
-  }
+  // destination words dw[0, nw) hold the row at bytes [lo, end)
+  const uint32_t lo = uint32_t(reinterpret_cast<uintptr_t>(d) & 15);
+  uint4 *dw = reinterpret_cast<uint4 *>(d - lo);
+  const uint32_t end = lo + n;
+  const uint32_t nw = (end + 15) >> 4;
+  // destination byte x of the words comes from source byte aw + o + x
+  const char *s0 = s - lo;
+  const uint32_t o = uint32_t(reinterpret_cast<uintptr_t>(s0) & 15);
+  const uint4 *aw = reinterpret_cast<const uint4 *>(s0 - o);
+  const uint32_t j_first = (o + lo) >> 4, j_last = (o + end - 1) >> 4;
   const uint32_t q = o >> 2, sh = (o & 3) * 8;
   constexpr unsigned kMask = L == 32 ? 0xffffffffu : ((1u << L) - 1u);
   const unsigned mask = kMask << (threadIdx.x & 31 & ~(L - 1));
-  // every lane of a group runs the same number of passes (uniform `nb`)
-  for (uint32_t base = 0; base < nb; base += L * K) {
-    const uint32_t j0 = base + lane * K;
+  const uint32_t from = (lane + 1) & (L - 1);
+  // every lane of a group runs the same number of passes (uniform `nw`)
+  for (uint32_t base = 0; base < nw; base += L * K) {
+    // a[k] = source word base + k*L + lane; lane 0 also loads the word after
+    // the pass, base + K*L
     uint4 a[K + 1];
 #pragma unroll
-    for (int k = 0; k < K; ++k)
-      a[k] = (j0 + k <= nb) ? __ldg(aw + j0 + k) : make_uint4(0, 0, 0, 0);
-    a[K].x = __shfl_down_sync(mask, a[0].x, 1, L);
-    a[K].y = __shfl_down_sync(mask, a[0].y, 1, L);
-    a[K].z = __shfl_down_sync(mask, a[0].z, 1, L);
-    a[K].w = __shfl_down_sync(mask, a[0].w, 1, L);
-    if (lane == L - 1 && j0 + K <= nb)
-      a[K] = __ldg(aw + j0 + K);
+    for (int k = 0; k < K; ++k) {
+      const uint32_t j = base + k * L + lane;
+      a[k] = (j >= j_first && j <= j_last) ? __ldg(aw + j) : make_uint4(0, 0, 0, 0);
+    }
+    {
+      const uint32_t j = base + K * L;
+      a[K] = (lane == 0 && j >= j_first && j <= j_last) ? __ldg(aw + j)
+                                                         : make_uint4(0, 0, 0, 0);
+    }
 #pragma unroll
-    for (int k = 0; k < K; ++k)
-      if (j0 + k < nb)
-        dw[j0 + k] = realign(a[k], a[k + 1], q, sh);
+    for (int k = 0; k < K; ++k) {
+      // the word after lane l's word k is lane l+1's word k, and for the
+      // group's last lane it is lane 0's word k+1
+      const uint4 send = lane == 0 ? a[k + 1] : a[k];
+      uint4 next;
+      next.x = __shfl_sync(mask, send.x, from, L);
+      next.y = __shfl_sync(mask, send.y, from, L);
+      next.z = __shfl_sync(mask, send.z, from, L);
+      next.w = __shfl_sync(mask, send.w, from, L);
+      const uint32_t j = base + k * L + lane;
+      if (j < nw) {
+        const uint4 v = realign(a[k], next, q, sh);
+        const uint32_t b0 = j == 0 ? lo : 0;
+        const uint32_t b1 = j == nw - 1 ? end - 16 * j : 16;
+        if (b0 == 0 && b1 == 16)
+          dw[j] = v;
+        else
+          store_part(reinterpret_cast<char *>(dw + j), v, b0, b1);
+      }
+    }
   }
 }
 
