@@ -64,7 +64,7 @@ extern "C" int64_t tempi_counter(const char *name) {
   C(lib_pack) C(lib_unpack) C(cached_types) C(send_device) C(send_oneshot)
   C(send_staged) C(send_lib) C(recv_device) C(recv_oneshot) C(recv_staged)
   C(recv_lib) C(isend_managed) C(irecv_managed) C(dispatch_hit)
-  C(dispatch_miss) C(slab_hits) C(slab_misses) C(slab_bytes)
+  C(dispatch_miss) C(slab_hits) C(slab_misses) C(slab_bytes) C(host_link_copies)
 #undef C
   return -1;
 }

@@ -47,6 +47,7 @@ struct Counters {
   std::atomic<int64_t> dispatch_hit{0}, dispatch_miss{0};
   std::atomic<int64_t> slab_hits{0}, slab_misses{0}, slab_bytes{0};
   std::atomic<int64_t> cached_types{0};
+  std::atomic<int64_t> host_link_copies{0};
 };
 Counters &counters();
 

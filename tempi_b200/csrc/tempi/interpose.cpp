@@ -9,7 +9,10 @@
 //  * a committed type that TEMPI cannot describe goes to the library instead
 //    of dereferencing a null packer;
 //  * once TEMPI has taken a call onto the GPU path it never falls back to a
-//    CPU copy: a CUDA failure is returned as MPI_ERR_OTHER.
+//    CPU copy: a CUDA failure is returned as MPI_ERR_OTHER;
+//  * a contiguous run of at least 8 MiB between two pinned host buffers goes
+//    through the copy engines (hostlink.cpp), strided ones through the
+//    kernels.
 
 #include "dispatch.hpp"
 #include "runtime.hpp"
@@ -28,6 +31,17 @@ int to_mpi(int e) {
   case TEMPI_ERR_NO_MEM: return MPI_ERR_NO_MEM;
   default: return MPI_ERR_OTHER;
   }
+}
+
+// Both buffers pinned host memory and the objects one contiguous run: the
+// copy engines move it across the host link (hostlink.cpp).
+bool use_host_link(const PtrInfo &a, const PtrInfo &b, const tempi_desc &d,
+                   int64_t count) {
+  if (!env().host_link_dma || a.is_device || b.is_device)
+    return false;
+  if (int64_t(count) * d.size < kHostLinkMinBytes)
+    return false;
+  return contiguous_run(d, count) == int64_t(count) * d.size;
 }
 
 void on_init() {
@@ -117,9 +131,17 @@ int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
   if (*position < 0 || *position + bytes > int64_t(outsize))
     return MPI_ERR_TRUNCATE;
   cudaStream_t s = pack_stream();
-  tempi_config cfg = choose_config(*r, incount, !in.is_device, !out.is_device);
-  int e = tempi_pack(&r->desc, in.device_ptr, incount,
-                     static_cast<char *>(out.device_ptr) + *position, &cfg, s);
+  int e;
+  if (use_host_link(in, out, r->desc, incount)) {
+    e = host_link_copy(static_cast<char *>(outbuf) + *position,
+                       static_cast<const char *>(inbuf) + r->desc.start,
+                       size_t(bytes), s);
+  } else {
+    tempi_config cfg =
+        choose_config(*r, incount, !in.is_device, !out.is_device);
+    e = tempi_pack(&r->desc, in.device_ptr, incount,
+                   static_cast<char *>(out.device_ptr) + *position, &cfg, s);
+  }
   if (!e) {
     cudaError_t ce = cudaStreamSynchronize(s);
     if (ce != cudaSuccess)
@@ -156,10 +178,18 @@ int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
   if (*position < 0 || *position + bytes > int64_t(insize))
     return MPI_ERR_TRUNCATE;
   cudaStream_t s = pack_stream();
-  tempi_config cfg = choose_config(*r, outcount, !out.is_device, !in.is_device);
-  int e = tempi_unpack(&r->desc,
-                       static_cast<const char *>(in.device_ptr) + *position,
-                       outcount, out.device_ptr, &cfg, s);
+  int e;
+  if (use_host_link(in, out, r->desc, outcount)) {
+    e = host_link_copy(static_cast<char *>(outbuf) + r->desc.start,
+                       static_cast<const char *>(inbuf) + *position,
+                       size_t(bytes), s);
+  } else {
+    tempi_config cfg =
+        choose_config(*r, outcount, !out.is_device, !in.is_device);
+    e = tempi_unpack(&r->desc,
+                     static_cast<const char *>(in.device_ptr) + *position,
+                     outcount, out.device_ptr, &cfg, s);
+  }
   if (!e) {
     cudaError_t ce = cudaStreamSynchronize(s);
     if (ce != cudaSuccess)

@@ -46,6 +46,8 @@ void read_env() {
   }
   if (const char *s = std::getenv("TEMPI_WAIT_TIMEOUT_S"))
     e.wait_timeout_s = std::atof(s);
+  if (const char *s = std::getenv("TEMPI_HOST_LINK"))
+    e.host_link_dma = std::string(s) != "kernel";
   if (const char *cd = std::getenv("TEMPI_CACHE_DIR")) {
     e.cache_dir = cd;
   } else if (const char *x = std::getenv("XDG_CACHE_HOME")) {
@@ -92,6 +94,18 @@ cudaStream_t pack_stream() {
     }
   }
   return g_stream;
+}
+
+cudaStream_t link_stream() {
+  static cudaStream_t h = nullptr;
+  std::lock_guard<std::mutex> l(g_dev_mu);
+  if (!h) {
+    if (cudaStreamCreateWithFlags(&h, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      h = nullptr;
+    }
+  }
+  return h;
 }
 
 PtrInfo classify(const void *p) {

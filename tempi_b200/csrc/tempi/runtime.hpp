@@ -26,6 +26,9 @@ struct Env {
   Dispatch dispatch = Dispatch::LEARNED; // TEMPI_DISPATCH=learned|table|exhaustive|heuristic
   std::string cache_dir;     // TEMPI_CACHE_DIR
   double wait_timeout_s = 30; // TEMPI_WAIT_TIMEOUT_S: bound on MPI_Wait polling
+  // TEMPI_HOST_LINK=kernel: contiguous runs between pinned host buffers go
+  // through the kernels too, instead of the copy-engine pipeline
+  bool host_link_dma = true;
 };
 const Env &env();
 void read_env(); // re-read the environment (MPI_Init does this)
@@ -56,6 +59,9 @@ void release_type(MPI_Datatype t);
 // Lazily creates TEMPI's non-blocking stream on the current device
 // (reference kernStream, src/internal/streams.cpp:19-28).
 cudaStream_t pack_stream();
+// A second non-blocking stream, for work that runs beside pack_stream()
+// (the copy-engine pipeline's device-to-host half).
+cudaStream_t link_stream();
 bool cuda_available();
 
 // Where a pointer lives.  device_ptr is what a kernel should use.
@@ -74,6 +80,17 @@ enum class Space { DEVICE, HOST_MAPPED };
 void *slab_alloc(Space s, size_t bytes);
 void slab_free(Space s, void *p);
 void slab_release_all();
+
+// ---- copy-engine path between pinned host buffers -------------------------
+// Bytes of the one contiguous run that `incount` objects of `d` describe, or
+// -1 when they describe more than one run.
+int64_t contiguous_run(const tempi_desc &d, int64_t incount);
+// Smallest run worth the copy-engine pipeline.
+constexpr int64_t kHostLinkMinBytes = int64_t(8) << 20;
+// Copy `n` bytes from pinned host `src` to pinned host `dst` through device
+// staging with the copy engines, both link directions busy at once; enqueued
+// on `s` and on link_stream(), and synchronised before it returns.
+int host_link_copy(void *dst, const void *src, size_t n, cudaStream_t s);
 
 // ---- event pool (reference src/internal/events.cpp:17-86) -----------------
 cudaEvent_t event_acquire();

@@ -171,6 +171,60 @@ def test_pack_into_pinned_host(cuda, mpi_init):
     assert out.numpy().tobytes() == T.pack(ty.o, src_np, 2).tobytes()
 
 
+@pytest.mark.parametrize("path", ["dma", "kernel"])
+@pytest.mark.parametrize("shape", ["rows", "contiguous"])
+def test_host_to_host_contiguous_run(cuda, mpi_init, path, shape):
+    """Pinned host typed and packed buffers with objects that form one
+    contiguous run (whole rows of a subarray at a start offset; three
+    adjacent contiguous objects): the copy-engine pipeline (TEMPI_HOST_LINK
+    unset) and the kernels (TEMPI_HOST_LINK=kernel) write the same bytes as
+    the oracle, at an odd packed position, and the unpack leaves every byte
+    outside the run alone."""
+    import os
+
+    import torch
+
+    if shape == "rows":  # one object: rows 17..3016 of 4096, 12,288,000 B
+        ty = H.subarray([4096, 1024], [3000, 1024], [17, 0], mpi.ORDER_C,
+                        H.named("FLOAT")).commit()
+        count = 1
+    else:  # three adjacent objects of 1,000,003 floats
+        ty = H.contiguous(1000003, H.named("FLOAT")).commit()
+        count = 3
+    assert ty.o.size * count >= 8 << 20
+    old = os.environ.get("TEMPI_HOST_LINK")
+    if path == "kernel":
+        os.environ["TEMPI_HOST_LINK"] = "kernel"
+    else:
+        os.environ.pop("TEMPI_HOST_LINK", None)
+    _lib.tempi().tempi_reload_env()
+    try:
+        src_np = H.splitmix_bytes(ty.o.extent * count, 21)
+        src = torch.from_numpy(src_np).pin_memory()
+        pos0 = 5
+        packed = torch.zeros(ty.o.size * count + pos0 + 3, dtype=torch.uint8).pin_memory()
+        n0 = _lib.counter("host_link_copies")
+        err, pos = mpi.Pack(src.data_ptr(), count, ty.h, packed.data_ptr(), packed.numel(), pos0)
+        assert err == 0 and pos == pos0 + ty.o.size * count
+        want = T.pack(ty.o, src_np, count)
+        assert packed.numpy()[pos0:pos].tobytes() == want.tobytes()
+        assert not packed.numpy()[:pos0].any() and not packed.numpy()[pos:].any()
+        back = torch.full_like(src, 0xAA).pin_memory()
+        err, upos = mpi.Unpack(packed.data_ptr(), packed.numel(), back.data_ptr(), count, ty.h, pos0)
+        assert err == 0 and upos == pos
+        exp = np.full_like(src_np, 0xAA)
+        T.unpack(ty.o, want, exp, count)
+        assert back.numpy().tobytes() == exp.tobytes()
+        used = _lib.counter("host_link_copies") - n0
+        assert used == (2 if path == "dma" else 0)
+    finally:
+        if old is None:
+            os.environ.pop("TEMPI_HOST_LINK", None)
+        else:
+            os.environ["TEMPI_HOST_LINK"] = old
+        _lib.tempi().tempi_reload_env()
+
+
 @pytest.mark.parametrize("kernel", [1, 2])
 @pytest.mark.parametrize("width", [1, 2, 4, 8, 16])
 @pytest.mark.parametrize("threads", [64, 256, 512])
