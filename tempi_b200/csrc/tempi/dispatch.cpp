@@ -271,6 +271,16 @@ uint64_t config_key(int64_t incount, bool src_host, bool dst_host) {
 
 } // namespace
 
+bool contiguous_staged_faster(int64_t bytes) {
+  std::lock_guard<std::mutex> l(g_mu);
+  const Table &t = g_table;
+  if (!t.loaded)
+    return false;
+  const double staged = table_1d(t.d2h, bytes) + table_1d(t.pp_host, bytes) +
+                        table_1d(t.h2d, bytes);
+  return staged < table_1d(t.pp_dev, bytes);
+}
+
 bool eligible(const tempi_desc &d, int64_t incount, int k) {
   Geometry g;
   bool empty = false;

@@ -37,6 +37,12 @@ void features(const tempi_desc &d, int64_t incount, bool src_host,
 // Transfer method for `count` objects of a committed type (cached per
 // packed byte count in the record).  TEMPI_DATATYPE_* overrides everything.
 Method choose_method(TypeRecord &r, int count);
+// TEMPI_CONTIGUOUS_AUTO for a contiguous device buffer of `bytes`: whether
+// staging through host memory (copy to host, host send, copy back) beats a
+// send straight from device memory, by the measured tables (reference
+// SendRecv1D::send/recv, src/internal/sender.cpp:63-88).  False without
+// tables.
+bool contiguous_staged_faster(int64_t bytes);
 
 // Kernel configuration for one pack/unpack launch of a committed type.
 tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,

@@ -48,6 +48,7 @@ struct Counters {
   std::atomic<int64_t> slab_hits{0}, slab_misses{0}, slab_bytes{0};
   std::atomic<int64_t> cached_types{0};
   std::atomic<int64_t> host_link_copies{0};
+  std::atomic<int64_t> send_contig_staged{0}, recv_contig_staged{0};
 };
 Counters &counters();
 

@@ -44,9 +44,29 @@ bool use_host_link(const PtrInfo &a, const PtrInfo &b, const tempi_desc &d,
   return contiguous_run(d, count) == int64_t(count) * d.size;
 }
 
+// A contiguous device buffer goes through host staging under
+// TEMPI_CONTIGUOUS_STAGED always, under TEMPI_CONTIGUOUS_AUTO when the
+// measured tables say staging is faster (reference types_init and
+// type_commit.cpp:37-58 choose SendRecv1DStaged / SendRecv1D the same way);
+// otherwise the library sends it as it is.
+bool contiguous_staged(const TypeRecord *r, const PtrInfo &p, int count) {
+  if (!r || !r->packable || r->desc.ndims != 0 || count <= 0 || !p.is_device)
+    return false;
+  if (env().contiguous == Contiguous::STAGED)
+    return true;
+  return env().contiguous == Contiguous::AUTO &&
+         contiguous_staged_faster(int64_t(count) * r->desc.size);
+}
+
 void on_init() {
   read_env();
   dispatch_init();
+  // the named types a contiguous send uses are known from the start, as in
+  // the reference's types_init (src/internal/types.cpp:723-755, called from
+  // src/init.cpp:63 unless TEMPI is disabled)
+  if (!env().disable)
+    for (MPI_Datatype t : {MPI_BYTE, MPI_FLOAT, MPI_DOUBLE})
+      commit_type(t);
 }
 
 void on_finalize() {
@@ -213,8 +233,7 @@ int MPI_Send(const void *buf, int count, MPI_Datatype datatype, int dest,
     Method m = choose_method(*r, count);
     return send_strided(*r, m, p.device_ptr, count, dest, tag, comm);
   }
-  if (r && r->packable && r->desc.ndims == 0 && count > 0 &&
-      env().contiguous == Contiguous::STAGED && p.is_device) {
+  if (contiguous_staged(r, p, count)) {
     return send_contiguous_staged(buf, count, datatype,
                                   int64_t(count) * r->desc.size, dest, tag,
                                   comm);
@@ -235,8 +254,7 @@ int MPI_Recv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
     Method m = choose_method(*r, count);
     return recv_strided(*r, m, p.device_ptr, count, source, tag, comm, status);
   }
-  if (r && r->packable && r->desc.ndims == 0 && count > 0 &&
-      env().contiguous == Contiguous::STAGED && p.is_device) {
+  if (contiguous_staged(r, p, count)) {
     return recv_contiguous_staged(buf, count, datatype,
                                   int64_t(count) * r->desc.size, source, tag,
                                   comm, status);

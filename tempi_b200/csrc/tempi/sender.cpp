@@ -186,6 +186,7 @@ int send_contiguous_staged(const void *buf, int count, MPI_Datatype dt,
   int merr = e == cudaSuccess ? libmpi.Send(h, count, dt, dest, tag, comm)
                               : to_mpi(cuda_error(e, "staged copy"));
   slab_free(Space::HOST_MAPPED, h);
+  counters().send_contig_staged++;
   return merr;
 }
 
@@ -202,6 +203,7 @@ int recv_contiguous_staged(void *buf, int count, MPI_Datatype dt,
       merr = to_mpi(cuda_error(e, "staged copy"));
   }
   slab_free(Space::HOST_MAPPED, h);
+  counters().recv_contig_staged++;
   return merr;
 }
 

@@ -119,7 +119,9 @@ def test_c_application_links_through_rtld_next(tmp_path):
 
 def test_env_disable_and_no_pack(tmp_path):
     """TEMPI_DISABLE / TEMPI_NO_TYPE_COMMIT are read at MPI_Init (any value,
-    even empty, counts); with them set nothing is cached at commit."""
+    even empty, counts); with them set nothing is cached at commit.  MPI_Init
+    itself caches MPI_BYTE, MPI_FLOAT and MPI_DOUBLE unless TEMPI is
+    disabled (the reference's types_init)."""
     code = (
         "import sys; sys.path.insert(0, %r)\n"
         "from tempi_b200 import mpi\n"
@@ -128,7 +130,7 @@ def test_env_disable_and_no_pack(tmp_path):
         "t = mpi.Type_vector(4, 2, 8, mpi.BYTE); mpi.Type_commit(t)\n"
         "print(_lib.counter('cached_types'))\n" % ROOT
     )
-    for var, want in (("TEMPI_DISABLE", "0"), ("TEMPI_NO_TYPE_COMMIT", "0"), ("UNSET_X", "1")):
+    for var, want in (("TEMPI_DISABLE", "0"), ("TEMPI_NO_TYPE_COMMIT", "3"), ("UNSET_X", "4")):
         env = dict(os.environ, **{var: ""})
         r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
                            env=env, timeout=120)

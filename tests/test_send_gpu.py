@@ -132,3 +132,42 @@ def test_wait_without_sender_times_out(cuda, mpi_init):
         _lib.tempi().tempi_reload_env()
     # still usable
     test_tags_match_in_order(torch.device("cuda"), mpi_init)
+
+
+@pytest.mark.parametrize("mode", ["STAGED", "AUTO", "NONE"])
+def test_contiguous_device_send(cuda, mpi_init, mode):
+    """Contiguous device buffers (named MPI_FLOAT and MPI_BYTE, a derived
+    contiguous type): TEMPI_CONTIGUOUS_STAGED stages every send and receive
+    through host memory (reference SendRecv1DStaged, sender.cpp:34-61),
+    TEMPI_CONTIGUOUS_AUTO stages when the measured tables say it is faster
+    (SendRecv1D, sender.cpp:63-88), and without either the library sends the
+    device buffer as it is.  Every received byte must match."""
+    import torch
+
+    var = {"STAGED": "TEMPI_CONTIGUOUS_STAGED", "AUTO": "TEMPI_CONTIGUOUS_AUTO"}.get(mode)
+    if var:
+        os.environ[var] = ""
+    _lib.tempi().tempi_reload_env()
+    try:
+        dbl = H.contiguous(77, H.named("DOUBLE")).commit()
+        for t, count, size in ((mpi.FLOAT, 3000, 4), (dbl.h, 5, 616), (mpi.BYTE, 1 << 20, 1)):
+            src_np = H.splitmix_bytes(count * size, count)
+            src, dst = dev(src_np), dev(np.zeros_like(src_np))
+            torch.cuda.synchronize()
+            s0 = _lib.counter("send_contig_staged")
+            r0 = _lib.counter("recv_contig_staged")
+            assert mpi.Send(src.data_ptr(), count, t, tag=7) == 0
+            assert mpi.Recv(dst.data_ptr(), count, t, tag=7)[0] == 0
+            assert dst.cpu().numpy().tobytes() == src_np.tobytes()
+            ds = _lib.counter("send_contig_staged") - s0
+            dr = _lib.counter("recv_contig_staged") - r0
+            if mode == "STAGED":
+                assert ds == 1 and dr == 1
+            elif mode == "NONE":
+                assert ds == 0 and dr == 0
+            else:  # the same model decides both sides of the same byte count
+                assert ds == dr and ds in (0, 1)
+    finally:
+        if var:
+            os.environ.pop(var, None)
+        _lib.tempi().tempi_reload_env()
