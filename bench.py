@@ -830,6 +830,100 @@ def run_profile(args):
                       "device_bytes": int(src.numel() * 2 + packed.numel())}))
 
 
+def run_profile_halo(args):
+    """A small case for ncu: the batched pack of the 256^3-double, radius-2
+    halo (26 regions, one launch), launched --profile-reps times."""
+    import torch
+
+    from tempi_b200 import halo, mpi
+
+    assert mpi.Init() == 0
+    g = halo.Grid((256, 256, 256), 2)
+    data = torch.randint(0, 256, (g.nbytes,), dtype=torch.uint8, device="cuda")
+    packed = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
+    b = halo.HaloBatch([g], [data.data_ptr()], [packed.data_ptr()], unpack=args.profile_unpack)
+    torch.cuda.synchronize()
+    for _ in range(args.profile_reps):
+        b.launch()
+    torch.cuda.synchronize()
+    b.close()
+    print(json.dumps({"profile": "halo 256^3 doubles r=2", "regions": 26,
+                      "packed_bytes": g.packed_bytes, "device_bytes": g.nbytes + g.packed_bytes,
+                      "unpack": bool(args.profile_unpack)}))
+
+
+def run_host_link(args):
+    """Host-link rates on this machine: the copy engines one way and both
+    ways, the word kernel reading, writing and copying pinned host memory,
+    and the copy-engine pipeline MPI_Pack uses for contiguous runs between
+    two pinned host buffers (256 MiB each)."""
+    import torch
+
+    from tempi_b200 import _lib, mpi
+
+    assert mpi.Init() == 0
+    lib = _lib.tempi()
+    n = 256 << 20
+    ha = torch.randint(0, 256, (n,), dtype=torch.uint8).pin_memory()
+    hb = torch.empty(n, dtype=torch.uint8).pin_memory()
+    da = torch.empty(n, dtype=torch.uint8, device="cuda")
+    db = torch.empty(n, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.ExternalStream(_tempi_stream())
+    s2 = torch.cuda.Stream()
+    reps = max(3, args.profile_reps)
+
+    def gbs(fn, nbytes):
+        fn()
+        torch.cuda.synchronize()
+        return round(nbytes / time_events(torch, st, fn, reps) / 1e6, 1)
+
+    def h2d():
+        with torch.cuda.stream(st):
+            da.copy_(ha, non_blocking=True)
+
+    def d2h():
+        with torch.cuda.stream(st):
+            hb.copy_(db, non_blocking=True)
+
+    def both():
+        e0 = torch.cuda.Event()
+        e0.record(st)
+        s2.wait_event(e0)
+        with torch.cuda.stream(st):
+            da.copy_(ha, non_blocking=True)
+        with torch.cuda.stream(s2):
+            hb.copy_(db, non_blocking=True)
+        e1 = torch.cuda.Event()
+        e1.record(s2)
+        st.wait_event(e1)
+
+    t = mpi.Type_contiguous(n, mpi.BYTE)
+    assert mpi.Type_commit(t) == 0
+    err, d = mpi.describe(t)
+    assert err == 0
+
+    def kernel(src, dst):
+        return lambda: _lib.check(lib.tempi_pack(ctypes.byref(d), src.data_ptr(), 1,
+                                                 dst.data_ptr(), None, st.cuda_stream))
+
+    def pipeline():
+        err, _ = mpi.Pack(ha.data_ptr(), 1, t, hb.data_ptr(), n)
+        assert err == 0
+
+    out = {
+        "copy_engine_h2d": gbs(h2d, n), "copy_engine_d2h": gbs(d2h, n),
+        "copy_engines_both_ways_each": round(gbs(both, 2 * n) / 2, 1),
+        "kernel_reads_host": gbs(kernel(ha, da), n),
+        "kernel_writes_host": gbs(kernel(da, hb), n),
+        "kernel_host_to_host_each_way": gbs(kernel(ha, hb), n),
+    }
+    dma0 = _lib.counter("host_link_copies")
+    out["mpi_pack_host_to_host_each_way"] = gbs(pipeline, n)
+    out["mpi_pack_used_copy_engines"] = _lib.counter("host_link_copies") > dma0
+    assert torch.equal(ha, hb)
+    print(json.dumps({"host_link_gbs_per_direction": out, "bytes": n}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -847,8 +941,16 @@ def main():
     ap.add_argument("--profile-incount", type=int, default=2)
     ap.add_argument("--profile-reps", type=int, default=3)
     ap.add_argument("--profile-unpack", action="store_true")
+    ap.add_argument("--profile-halo", action="store_true",
+                    help="run only the batched halo kernel (for ncu)")
+    ap.add_argument("--host-link", action="store_true",
+                    help="measure the host-link rates and exit")
     args = ap.parse_args()
-    if args.profile_point:
+    if args.host_link:
+        run_host_link(args)
+    elif args.profile_halo:
+        run_profile_halo(args)
+    elif args.profile_point:
         run_profile(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -38,9 +38,10 @@ int host_link_copy(void *dst, const void *src, size_t n, cudaStream_t s) {
   cudaStream_t h = link_stream();
   if (!h)
     return set_error(TEMPI_ERR_CUDA, "host link: no helper stream");
-  // at least 2 * kStages chunks so both directions overlap for most of it
-  const size_t chunk =
-      std::min(kMaxChunk, std::max(kMinChunk, n / (2 * kStages) + 1));
+  // at least 2 * kStages chunks so both directions overlap for most of it;
+  // whole MiB, so every staging slot and chunk offset stays aligned
+  const size_t want = (n / (2 * kStages) + kMinChunk - 1) / kMinChunk * kMinChunk;
+  const size_t chunk = std::min(kMaxChunk, std::max(kMinChunk, want));
   char *stage = static_cast<char *>(slab_alloc(Space::DEVICE, kStages * chunk));
   if (!stage)
     return set_error(TEMPI_ERR_NO_MEM, "host link: staging allocation failed");
