@@ -624,8 +624,8 @@ def dispatch_sample(torch, n=200, seed=777):
 
     lib = _lib.tempi()
     rng = np.random.default_rng(seed)
-    times = (ctypes.c_float * 12)()
-    learned, fixed, best = [], [], []
+    times = (ctypes.c_float * DT.N_MEAS)()
+    learned, fixed, best, where = [], [], [], []
     t0 = time.time()
     while len(best) < n and time.time() - t0 < 60:
         d, incount, th, ph = DT.random_layout(rng)
@@ -634,22 +634,30 @@ def dispatch_sample(torch, n=200, seed=777):
         size = d.size * incount
         reps = 3 if size < (1 << 20) else 2 if size < (64 << 20) else 1
         _lib.check(lib.tempi_measure(ctypes.byref(d), incount, int(th), int(ph), 1, reps, times))
-        ci = ctypes.c_int(-1)
-        mi = ctypes.c_int(0)
+        pc, uc, mi = ctypes.c_int(-1), ctypes.c_int(-1), ctypes.c_int(0)
         if lib.tempi_dispatch_choose(ctypes.byref(d), incount, int(th), int(ph), 0,
-                                     ctypes.byref(ci), ctypes.byref(mi), None, None):
+                                     ctypes.byref(pc), ctypes.byref(uc), ctypes.byref(mi),
+                                     None, None):
             return {"error": _lib.last_error()}
         t = np.frombuffer(times, np.float32)
-        cand = t[:8]
-        best.append(float(np.nanmin(cand)))
-        learned.append(float(cand[ci.value]))
-        fixed.append(float(t[11]))
+        tp = t[DT.PACK:DT.PACK + DT.N_CFG]
+        tu = t[DT.UNPACK:DT.UNPACK + DT.N_CFG]
+        best.append(float(np.nanmin(tp) + np.nanmin(tu)))
+        learned.append(float(tp[pc.value] + tu[uc.value]))
+        fixed.append(float(t[DT.FIXED_PACK] + t[DT.FIXED_UNPACK]))
+        where.append((d.as_dict(), incount, bool(th), bool(ph), pc.value, uc.value))
     L, F, B = map(np.array, (learned, fixed, best))
+    worst = [{"us_learned": round(float(L[i]), 1), "us_best": round(float(B[i]), 1),
+              "layout": where[i][0], "incount": where[i][1], "typed_host": where[i][2],
+              "packed_host": where[i][3], "picks": where[i][4:]}
+             for i in np.argsort(-(L - B))[:3]]
     return {"layouts": len(B), "seed": seed,
             "learned_total_regret": round(float(L.sum() / B.sum() - 1), 4),
             "fixed_rules_total_regret": round(float(F.sum() / B.sum() - 1), 4),
             "learned_within_5pct": round(float(np.mean(L <= 1.05 * B)), 3),
-            "learned_mean_regret": round(float(np.mean(L / B - 1)), 4)}
+            "learned_mean_regret": round(float(np.mean(L / B - 1)), 4),
+            "exhaustive_total_us": round(float(B.sum()), 1),
+            "largest_losses": worst}
 
 
 def config1_bench(torch, mpi, reps=200):

@@ -170,7 +170,7 @@ _TEMPI_SIGS = {
     "tempi_measure": (c_int, [P(Desc), c_int64, c_int, c_int, c_int, c_int, c_void_p]),
     "tempi_dispatch_load": (c_int, [ctypes.c_char_p, ctypes.c_char_p]),
     "tempi_dispatch_choose": (c_int, [P(Desc), c_int64, c_int, c_int, c_int, P(c_int),
-                                      P(c_int), c_void_p, c_void_p]),
+                                      P(c_int), P(c_int), c_void_p, c_void_p]),
     "tempi_table_interp": (ctypes.c_double, [c_void_p, c_int, c_int, c_int64, c_int64]),
     "tempi_mlp_init": (c_int, [c_void_p, c_int, ctypes.c_uint64]),
     "tempi_mlp_train": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int, c_int,

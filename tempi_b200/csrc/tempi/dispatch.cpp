@@ -265,8 +265,10 @@ int pick(const float *mean, const float *spread, int lo, int hi, bool *trust,
   return best;
 }
 
-uint64_t config_key(int64_t incount, bool src_host, bool dst_host) {
-  return (uint64_t(incount) << 2) | (src_host ? 2 : 0) | (dst_host ? 1 : 0);
+uint64_t config_key(int64_t incount, bool src_host, bool dst_host,
+                    bool unpack) {
+  return (uint64_t(incount) << 3) | (unpack ? 4 : 0) | (src_host ? 2 : 0) |
+         (dst_host ? 1 : 0);
 }
 
 } // namespace
@@ -342,11 +344,12 @@ tempi_config choose_config(const tempi_desc &d, int64_t incount) {
 }
 
 tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
-                           bool dst_host) {
+                           bool dst_host, bool unpack) {
   const Dispatch mode = env().dispatch;
   if (mode == Dispatch::HEURISTIC || mode == Dispatch::TABLE || g_measuring)
     return tempi_config{};
-  const uint64_t key = config_key(incount, src_host, dst_host);
+  const uint64_t key = config_key(incount, src_host, dst_host, unpack);
+  const int lo = unpack ? kUnpackOut : kPackOut;
   {
     std::lock_guard<std::mutex> l(g_mu);
     auto it = r.configs.find(key);
@@ -365,7 +368,7 @@ tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
     float f[TEMPI_MLP_IN], mean[TEMPI_MLP_OUT], spread[TEMPI_MLP_OUT];
     features(r.desc, incount, src_host, dst_host, f);
     if (predict(f, mean, spread) == TEMPI_OK)
-      choice = pick(mean, spread, 0, kNumConfigs, &trust, ok);
+      choice = pick(mean, spread, lo, lo + kNumConfigs, &trust, ok) - lo;
   }
   if (mode == Dispatch::EXHAUSTIVE || (choice >= 0 && !trust)) {
     float t[kMeasured];
@@ -373,9 +376,18 @@ tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
         TEMPI_OK) {
       int best = -1;
       for (int j = 0; j < kNumConfigs; ++j)
-        if (std::isfinite(t[j]) && (best < 0 || t[j] < t[best]))
+        if (std::isfinite(t[lo + j]) && (best < 0 || t[lo + j] < t[lo + best]))
           best = j;
       choice = best;
+      // the same measurement answers the other direction too
+      int other = -1;
+      const int lo2 = unpack ? kPackOut : kUnpackOut;
+      for (int j = 0; j < kNumConfigs; ++j)
+        if (std::isfinite(t[lo2 + j]) &&
+            (other < 0 || t[lo2 + j] < t[lo2 + other]))
+          other = j;
+      std::lock_guard<std::mutex> l(g_mu);
+      r.configs[config_key(incount, src_host, dst_host, !unpack)] = other;
     }
   }
   std::lock_guard<std::mutex> l(g_mu);
@@ -413,12 +425,12 @@ Method choose_method(TypeRecord &r, int count) {
     features(r.desc, count, false, false, f);
     bool trust = false;
     if (predict(f, mean, spread) == TEMPI_OK) {
-      const int j = pick(mean, spread, kNumConfigs, kNumConfigs + kNumMethods,
-                         &trust);
+      const int j =
+          pick(mean, spread, kMethodOut, kMethodOut + kNumMethods, &trust);
       // an untrusted prediction keeps the fixed rule: timing a transfer
       // needs a matching receive, which a send cannot arrange by itself
       if (trust)
-        m = Method(j - kNumConfigs + 1);
+        m = Method(j - kMethodOut + 1);
     }
   }
   std::lock_guard<std::mutex> l(g_mu);
@@ -430,7 +442,9 @@ void on_commit(TypeRecord &r) {
   if (!r.packable || r.desc.size == 0 || env().dispatch != Dispatch::LEARNED ||
       !g_model.loaded || g_measuring)
     return;
-  choose_config(r, 1, false, false); // cached for device-to-device packs
+  // cached for device-to-device packs and unpacks
+  choose_config(r, 1, false, false, false);
+  choose_config(r, 1, false, false, true);
 }
 
 void dispatch_init() {
@@ -472,11 +486,12 @@ extern "C" int tempi_dispatch_load(const char *model_path,
 
 extern "C" int tempi_dispatch_choose(const tempi_desc *d, int64_t incount,
                                      int src_host, int dst_host, int mode,
-                                     int *config_index, int *method,
-                                     float *predicted, float *spread) {
+                                     int *pack_config, int *unpack_config,
+                                     int *method, float *predicted,
+                                     float *spread) {
   if (!d)
     return set_error(TEMPI_ERR_ARG, "null descriptor");
-  int ci = -1, mi = int(Method::DEVICE);
+  int pc = -1, uc = -1, mi = int(Method::DEVICE);
   float f[TEMPI_MLP_IN], mean[TEMPI_MLP_OUT], sp[TEMPI_MLP_OUT];
   for (int j = 0; j < TEMPI_MLP_OUT; ++j)
     mean[j] = sp[j] = NAN;
@@ -490,16 +505,21 @@ extern "C" int tempi_dispatch_choose(const tempi_desc *d, int64_t incount,
     bool trust, ok[kNumConfigs];
     for (int k = 0; k < kNumConfigs; ++k)
       ok[k] = eligible(*d, incount, k);
-    ci = pick(mean, sp, 0, kNumConfigs, &trust, ok);
-    mi = pick(mean, sp, kNumConfigs, kNumConfigs + kNumMethods, &trust) -
-         kNumConfigs + 1;
+    pc = pick(mean, sp, kPackOut, kPackOut + kNumConfigs, &trust, ok) -
+         kPackOut;
+    uc = pick(mean, sp, kUnpackOut, kUnpackOut + kNumConfigs, &trust, ok) -
+         kUnpackOut;
+    mi = pick(mean, sp, kMethodOut, kMethodOut + kNumMethods, &trust) -
+         kMethodOut + 1;
   } else if (mode == 1) { // restated perf tables
     if (!g_table.loaded)
       return set_error(TEMPI_ERR_UNSUPPORTED, "no tables loaded");
     mi = int(table_method(int64_t(incount) * d->size, d->block));
-  } // mode 2: fixed rules (ci = -1: launch_geometry's choice, DEVICE)
-  if (config_index)
-    *config_index = ci;
+  } // mode 2: fixed rules (-1: launch_geometry's choice, DEVICE)
+  if (pack_config)
+    *pack_config = pc;
+  if (unpack_config)
+    *unpack_config = uc;
   if (method)
     *method = mi;
   for (int j = 0; j < TEMPI_MLP_OUT; ++j) {

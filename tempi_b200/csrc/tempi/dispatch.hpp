@@ -6,22 +6,29 @@
 // word size by a fixed rule.  Here a learned cost model (an FP32 MLP
 // ensemble, mlp.cu) predicts the time of every candidate -- eight kernel
 // configurations and three transfer methods -- from twelve features of the
-// object; the candidate with the smallest predicted time wins.  When the
-// ensemble disagrees about the winner, the candidates are timed for real
-// (exhaustive autotuning).  Choices are cached per type.
+// object; the candidate with the smallest predicted time wins, for a pack
+// and for an unpack separately.  When the ensemble disagrees about the
+// winner, the candidates are timed for real (exhaustive autotuning).
+// Choices are cached per type.
 #pragma once
 
 #include "runtime.hpp"
 
 namespace tempi {
 
-constexpr int kNumConfigs = 8; // model outputs 0..7
-constexpr int kNumMethods = 3; // model outputs 8..10: DEVICE, ONE_SHOT, STAGED
+constexpr int kNumConfigs = 8; // kernel configurations
+constexpr int kNumMethods = 3; // DEVICE, ONE_SHOT, STAGED
+// model outputs: pack with configuration k, unpack with configuration k,
+// self-send by method m
+constexpr int kPackOut = 0, kUnpackOut = kNumConfigs,
+              kMethodOut = 2 * kNumConfigs;
+static_assert(kMethodOut + kNumMethods == TEMPI_MLP_OUT, "model outputs");
 extern const tempi_config kCandidates[kNumConfigs];
-// measured entries: the model's 11 outputs, then the fixed rules' pack +
-// unpack time (the policy without the model)
-constexpr int kFixedRules = TEMPI_MLP_OUT;
-constexpr int kMeasured = TEMPI_MLP_OUT + 1;
+// measured entries: the model's outputs, then the fixed rules' pack and
+// unpack times (the policy without the model)
+constexpr int kFixedPack = TEMPI_MLP_OUT, kFixedUnpack = TEMPI_MLP_OUT + 1;
+constexpr int kMeasured = TEMPI_MEASURED;
+static_assert(kFixedUnpack + 1 == kMeasured, "measured entries");
 
 // Whether candidate configuration k suits `incount` objects of `d`: a warp
 // per row needs rows of at least 64 B, a shift group of L lanes rows of at
@@ -44,9 +51,11 @@ Method choose_method(TypeRecord &r, int count);
 // tables.
 bool contiguous_staged_faster(int64_t bytes);
 
-// Kernel configuration for one pack/unpack launch of a committed type.
+// Kernel configuration for one pack (unpack = false) or unpack launch of a
+// committed type; src_host / dst_host: the typed / packed buffer is host
+// memory.
 tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
-                           bool dst_host);
+                           bool dst_host, bool unpack);
 // ...and for an object with no record (the fixed rules)
 tempi_config choose_config(const tempi_desc &d, int64_t incount);
 
@@ -56,10 +65,10 @@ void on_commit(TypeRecord &r);
 // Load models from TEMPI_CACHE_DIR or next to the library (MPI_Init).
 void dispatch_init();
 
-// Time every candidate: times_us[0..7] = pack + unpack with each kernel
-// configuration, [8..10] = self-send round trip by each method, [11] = pack
-// + unpack by the fixed rules (NaN where not measured).  `what`: bit 0
-// configurations, bit 1 methods.
+// Time every candidate: times_us[0..7] = pack and [8..15] = unpack with each
+// kernel configuration, [16..18] = self-send round trip by each method,
+// [19] / [20] = pack / unpack by the fixed rules (NaN where not measured).
+// `what`: bit 0 configurations, bit 1 methods.
 int measure_candidates(const tempi_desc &d, int64_t incount, bool src_host,
                        bool dst_host, int what, int reps, float *times_us);
 

@@ -158,7 +158,7 @@ int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
                        size_t(bytes), s);
   } else {
     tempi_config cfg =
-        choose_config(*r, incount, !in.is_device, !out.is_device);
+        choose_config(*r, incount, !in.is_device, !out.is_device, false);
     e = tempi_pack(&r->desc, in.device_ptr, incount,
                    static_cast<char *>(out.device_ptr) + *position, &cfg, s);
   }
@@ -205,7 +205,7 @@ int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
                        size_t(bytes), s);
   } else {
     tempi_config cfg =
-        choose_config(*r, outcount, !out.is_device, !in.is_device);
+        choose_config(*r, outcount, !out.is_device, !in.is_device, true);
     e = tempi_unpack(&r->desc,
                      static_cast<const char *>(in.device_ptr) + *position,
                      outcount, out.device_ptr, &cfg, s);

@@ -125,15 +125,20 @@ int measure_candidates(const tempi_desc &d, int64_t incount, bool src_host,
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    // the fixed rules first (entry 11), then every eligible candidate.  The
-    // first timed pass doubles as the warm-up; a candidate more than 3x
-    // slower than the best so far keeps that one pass and is not repeated.
-    float best = INFINITY;
-    auto pass = [&](const tempi_config *cfg, int n) -> float {
+    // the fixed rules first, then every eligible candidate, packs and
+    // unpacks timed apart.  The first timed pass doubles as the warm-up; a
+    // candidate more than 3x slower than the best so far is not repeated
+    // `reps` times but timed once more, keeping the faster of its two
+    // passes (a first pass can carry one-off costs, such as the first
+    // launch of a kernel variant).
+    float best[2] = {INFINITY, INFINITY};
+    auto pass = [&](const tempi_config *cfg, bool unpack, int n) -> float {
       cudaEventRecord(a, g_stream);
       for (int r = 0; r < n; ++r) {
-        tempi_pack(&d, t_dev, incount, p_dev, cfg, g_stream);
-        tempi_unpack(&d, p_dev, incount, t_dev, cfg, g_stream);
+        if (unpack)
+          tempi_unpack(&d, p_dev, incount, t_dev, cfg, g_stream);
+        else
+          tempi_pack(&d, t_dev, incount, p_dev, cfg, g_stream);
       }
       cudaEventRecord(b, g_stream);
       cudaEventSynchronize(b);
@@ -142,15 +147,20 @@ int measure_candidates(const tempi_desc &d, int64_t incount, bool src_host,
       return 1e3f * ms / n;
     };
     for (int i = 0; i <= kNumConfigs; ++i) {
-      const int k = i == 0 ? kFixedRules : i - 1;
-      if (k != kFixedRules && !eligible(d, incount, k))
+      const int k = i == 0 ? -1 : i - 1; // -1: the fixed rules
+      if (k >= 0 && !eligible(d, incount, k))
         continue;
-      const tempi_config *cfg = k == kFixedRules ? nullptr : &kCandidates[k];
-      float t = pass(cfg, 1);
-      if (t <= 3 * best)
-        t = pass(cfg, reps);
-      times[k] = t;
-      best = std::min(best, t);
+      const tempi_config *cfg = k < 0 ? nullptr : &kCandidates[k];
+      for (int u = 0; u < 2; ++u) {
+        float t = pass(cfg, u == 1, 1);
+        if (t <= 3 * best[u])
+          t = pass(cfg, u == 1, reps);
+        else
+          t = std::min(t, pass(cfg, u == 1, 1));
+        times[k < 0 ? (u ? kFixedUnpack : kFixedPack)
+                    : (u ? kUnpackOut : kPackOut) + k] = t;
+        best[u] = std::min(best[u], t);
+      }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -180,9 +190,9 @@ int measure_candidates(const tempi_desc &d, int64_t incount, bool src_host,
                               std::chrono::steady_clock::now() - t0)
                               .count();
         if (r == 1)
-          times[kNumConfigs + m - 1] = 0;
+          times[kMethodOut + m - 1] = 0;
         if (r >= 1) // r == 0 is the warm-up
-          times[kNumConfigs + m - 1] += float(us / reps);
+          times[kMethodOut + m - 1] += float(us / reps);
       }
     }
     force_method(-1);

@@ -57,7 +57,8 @@ int send_strided(TypeRecord &r, Method m, const void *buf, int count, int dest,
                  int tag, MPI_Comm comm) {
   const int64_t bytes = int64_t(count) * r.desc.size;
   cudaStream_t s = pack_stream();
-  tempi_config cfg = choose_config(r, count, false, m == Method::ONESHOT);
+  tempi_config cfg = choose_config(r, count, false, m == Method::ONESHOT,
+                                   false);
   int err = TEMPI_OK;
   switch (m) {
   case Method::ONESHOT: {
@@ -113,7 +114,8 @@ int recv_strided(TypeRecord &r, Method m, void *buf, int count, int source,
                  int tag, MPI_Comm comm, MPI_Status *status) {
   const int64_t bytes = int64_t(count) * r.desc.size;
   cudaStream_t s = pack_stream();
-  tempi_config cfg = choose_config(r, count, false, m == Method::ONESHOT);
+  tempi_config cfg = choose_config(r, count, false, m == Method::ONESHOT,
+                                   true);
   int err = TEMPI_OK;
   switch (m) {
   case Method::ONESHOT: {
@@ -234,7 +236,8 @@ public:
       : m_(m) {
     const int64_t bytes = int64_t(count) * r.desc.size;
     cudaStream_t s = pack_stream();
-    tempi_config cfg = choose_config(r, count, false, m == Method::ONESHOT);
+    tempi_config cfg = choose_config(r, count, false, m == Method::ONESHOT,
+                                   false);
     ev_ = event_acquire();
     void *packed = nullptr;
     int terr = TEMPI_OK;
@@ -354,7 +357,8 @@ public:
       return err;
     const int64_t bytes = int64_t(count_) * r_.desc.size;
     cudaStream_t s = pack_stream();
-    tempi_config cfg = choose_config(r_, count_, false, m_ == Method::ONESHOT);
+    tempi_config cfg = choose_config(r_, count_, false, m_ == Method::ONESHOT,
+                                   true);
     int terr = TEMPI_OK;
     if (m_ == Method::ONESHOT) {
       terr = tempi_unpack(&r_.desc, host_dev_ptr(host_), count_, buf_, &cfg, s);

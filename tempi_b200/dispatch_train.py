@@ -9,13 +9,14 @@ equivalent:
    strides = inner extent x U[1,16] rounded to an alignment in
    {1,2,4,8,16}, totals 1 KiB - 256 MiB log-uniform, typed and packed
    buffers in device or mapped pinned host memory) and times every
-   candidate on each with tempi_measure: eight kernel configurations, the
-   fixed rules, and -- on a subset -- the three transfer methods;
-2. trains the cost model (a 5-member FP32 MLP ensemble, 12 -> 64 -> 64 -> 11)
+   candidate on each with tempi_measure: a pack and an unpack with each of
+   eight kernel configurations and with the fixed rules, and -- on a
+   subset -- the three transfer methods;
+2. trains the cost model (a 5-member FP32 MLP ensemble, 12 -> 64 -> 64 -> 19)
    on the GPU with tempi_mlp_train;
 3. measures the reference's table model on this machine (pack/unpack
    tables over 2^(2i+6) bytes x 2^j-byte blocks at a 512-byte stride,
-   self-send ping-pong tables), the comparison policy;
+   self-send ping-pong and host-copy tables), the comparison policy;
 4. evaluates on held-out layouts: prediction error, and the time regret of
    the learned choice, the table model and the fixed rules against
    exhaustive search;
@@ -42,8 +43,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 MODELS = os.path.join(HERE, "models")
 MODEL_FILE = "tempi_b200_dispatch.bin"
 TABLE_FILE = "tempi_b200_table.bin"
-N_CFG, N_METH, N_OUT, N_MEAS = 8, 3, 11, 12
-P = 5707
+N_CFG, N_METH = 8, 3
+PACK, UNPACK, METH = 0, N_CFG, 2 * N_CFG      # model output offsets
+N_OUT = 2 * N_CFG + N_METH                    # 19
+FIXED_PACK, FIXED_UNPACK = N_OUT, N_OUT + 1   # measured after the outputs
+N_MEAS = N_OUT + 2                            # 21
+P = (12 * 64 + 64) + (64 * 64 + 64) + (64 * N_OUT + N_OUT)
 
 
 def round_up(x, a):
@@ -168,7 +173,7 @@ def predict(params, members, X):
 def write_model(path, params_np, members, y_mean, y_std, gpu):
     with open(path, "wb") as fh:
         fh.write(b"TMLPv001")
-        fh.write(np.array([12, 64, 11, members], np.int32).tobytes())
+        fh.write(np.array([12, 64, N_OUT, members], np.int32).tobytes())
         fh.write(np.asarray(y_mean, np.float32).tobytes())
         fh.write(np.asarray(y_std, np.float32).tobytes())
         fh.write(np.asarray(params_np, np.float32).tobytes())
@@ -191,18 +196,30 @@ def measure_tables(log=print):
             d = _lib.Desc.make(0, count * 512, block, [count], [512])
             for ph, key in ((0, "dev"), (1, "host")):
                 _lib.check(lib.tempi_measure(ctypes.byref(d), 1, 0, ph, 1, 3, times))
-                t = float(times[11]) / 2
-                tabs["pack_" + key][i, j] = t
-                tabs["unpack_" + key][i, j] = t
-    # self-send ping-pong of contiguous bytes, device and host buffers
+                tabs["pack_" + key][i, j] = float(times[FIXED_PACK])
+                tabs["unpack_" + key][i, j] = float(times[FIXED_UNPACK])
+    # self-send ping-pong of contiguous bytes, device and host buffers, and
+    # copies between device and pinned host memory (the reference's d2h/h2d
+    # tables, measure_system.cu)
     N1 = 28
     pp_dev, pp_host = np.zeros(N1), np.zeros(N1)
+    d2h, h2d = np.zeros(N1), np.zeros(N1)
     dbuf = torch.zeros(1 << (N1 - 1), dtype=torch.uint8, device="cuda")
     dbuf2 = torch.zeros_like(dbuf)
     hbuf = np.zeros(1 << (N1 - 1), np.uint8)
     hbuf2 = np.zeros_like(hbuf)
+    pinned = torch.zeros(1 << (N1 - 1), dtype=torch.uint8).pin_memory()
     for i in range(N1):
         n = 1 << i
+        for arr, dst, src in ((d2h, pinned, dbuf), (h2d, dbuf2, pinned)):
+            reps = 5 if n < (1 << 20) else 2
+            dst[:n].copy_(src[:n])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                dst[:n].copy_(src[:n])
+                torch.cuda.synchronize()
+            arr[i] = 1e6 * (time.perf_counter() - t0) / reps
         for arr, (a, b) in ((pp_dev, (dbuf.data_ptr(), dbuf2.data_ptr())),
                             (pp_host, (hbuf.ctypes.data, hbuf2.ctypes.data))):
             reps = 5 if n < (1 << 20) else 2
@@ -214,15 +231,15 @@ def measure_tables(log=print):
                 mpi.Recv(b, n, mpi.BYTE, tag=91)
             arr[i] = 1e6 * (time.perf_counter() - t0) / reps
     log("  measured the table model's tables")
-    return tabs, pp_dev, pp_host
+    return tabs, pp_dev, pp_host, d2h, h2d
 
 
-def write_tables(path, tabs, pp_dev, pp_host):
+def write_tables(path, tabs, pp_dev, pp_host, d2h, h2d):
     with open(path, "wb") as fh:
         fh.write(b"TTABv001")
         NI, NJ = tabs["pack_dev"].shape
         fh.write(np.array([len(pp_dev), NI, NJ], np.int32).tobytes())
-        for a in (pp_dev, pp_host, pp_dev * 0, pp_dev * 0):  # d2h/h2d unused
+        for a in (pp_dev, pp_host, d2h, h2d):
             fh.write(np.asarray(a, np.float64).tobytes())
         for k in ("pack_dev", "unpack_dev", "pack_host", "unpack_host"):
             fh.write(np.asarray(tabs[k], np.float64).tobytes())
@@ -243,24 +260,46 @@ def evaluate(params, members, y_mean, y_std, X, T, meta, spread_limit=0.5):
     rows = np.arange(len(X))
     rep = {}
     # kernel configurations: measured (finite) entries are exactly the
-    # eligible candidates, which is all the dispatcher chooses among
-    elig = np.isfinite(T[:, :N_CFG])
-    ok = elig.any(1) & np.isfinite(T[:, 11])
-    best_cfg = np.where(elig, T[:, :N_CFG], np.inf)[ok].min(1)
-    ch = np.where(elig, mean[:, :N_CFG], np.inf)[ok].argmin(1)
-    t_learned = T[ok][np.arange(ok.sum()), ch]
-    sp = spread[ok][np.arange(ok.sum()), ch]
-    t_fallback = np.where(sp > spread_limit, best_cfg, t_learned)
+    # eligible candidates, which is all the dispatcher chooses among; a pack
+    # and an unpack are chosen separately
+    elig = np.isfinite(T[:, PACK:PACK + N_CFG]) & np.isfinite(T[:, UNPACK:UNPACK + N_CFG])
+    ok = elig.any(1) & np.isfinite(T[:, FIXED_PACK]) & np.isfinite(T[:, FIXED_UNPACK])
+    E, n_ok = elig[ok], int(ok.sum())
+    r = np.arange(n_ok)
+    tp, tu = T[ok, PACK:PACK + N_CFG], T[ok, UNPACK:UNPACK + N_CFG]
+    mp, mu = mean[ok, PACK:PACK + N_CFG], mean[ok, UNPACK:UNPACK + N_CFG]
+    sp_p, sp_u = spread[ok, PACK:PACK + N_CFG], spread[ok, UNPACK:UNPACK + N_CFG]
+    best_p = np.where(E, tp, np.inf).min(1)
+    best_u = np.where(E, tu, np.inf).min(1)
+    best_cfg = best_p + best_u
+    cp = np.where(E, mp, np.inf).argmin(1)
+    cu = np.where(E, mu, np.inf).argmin(1)
+    t_learned = tp[r, cp] + tu[r, cu]
+    fb_p, fb_u = sp_p[r, cp] > spread_limit, sp_u[r, cu] > spread_limit
+    t_fallback = np.where(fb_p, best_p, tp[r, cp]) + np.where(fb_u, best_u, tu[r, cu])
+    # one configuration for both directions, as a single prediction would pick
+    cj = np.where(E, 2.0 ** mp + 2.0 ** mu, np.inf).argmin(1)
+    t_joint = tp[r, cj] + tu[r, cj]
+    fixed = T[ok, FIXED_PACK] + T[ok, FIXED_UNPACK]
     rep["configs"] = {
-        "layouts": int(ok.sum()),
+        "layouts": n_ok,
         "learned": regret(t_learned, best_cfg),
         "learned_with_fallback": regret(t_fallback, best_cfg),
-        "fallback_rate": float(np.mean(sp > spread_limit)),
-        "fixed_rules": regret(T[ok, 11], best_cfg),
+        "fallback_rate": float(np.mean(fb_p | fb_u)),
+        "learned_one_config_for_both": regret(t_joint, best_cfg),
+        "fixed_rules": regret(fixed, best_cfg),
         "exhaustive_total_us": float(best_cfg.sum()),
         "learned_total_us": float(t_learned.sum()),
-        "fixed_rules_total_us": float(T[ok, 11].sum()),
+        "fixed_rules_total_us": float(fixed.sum()),
     }
+    host = (meta[ok, 1] > 0) | (meta[ok, 2] > 0)
+    if host.any():
+        rep["configs"]["host_buffers"] = {
+            "layouts": int(host.sum()),
+            "learned": regret(t_learned[host], best_cfg[host]),
+            "learned_one_config_for_both": regret(t_joint[host], best_cfg[host]),
+            "fixed_rules": regret(fixed[host], best_cfg[host]),
+        }
     y = np.log2(T[:, :N_OUT])
     obs = np.isfinite(y)
     err = np.abs(mean - np.where(obs, y, 0))[obs]
@@ -269,11 +308,11 @@ def evaluate(params, members, y_mean, y_std, X, T, meta, spread_limit=0.5):
         "p90_abs_rel_err": float(np.percentile(2 ** err - 1, 90)),
     }
     # transfer methods
-    okm = np.isfinite(T[:, N_CFG:N_CFG + N_METH]).all(1)
+    okm = np.isfinite(T[:, METH:METH + N_METH]).all(1)
     if okm.any():
-        tm = T[okm, N_CFG:N_CFG + N_METH]
+        tm = T[okm, METH:METH + N_METH]
         best_m = tm.min(1)
-        lm = mean[okm, N_CFG:N_CFG + N_METH].argmin(1)
+        lm = mean[okm, METH:METH + N_METH].argmin(1)
         rep["methods"] = {
             "layouts": int(okm.sum()),
             "learned": regret(tm[np.arange(len(tm)), lm], best_m),
@@ -289,12 +328,12 @@ def table_regret(X_rows_desc, T, okm_rows):
     lib = _lib.tempi()
     chosen = []
     for d, incount in X_rows_desc:
-        mi = ctypes.c_int(0)
-        ci = ctypes.c_int(0)
+        mi, pc, uc = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
         _lib.check(lib.tempi_dispatch_choose(ctypes.byref(d), incount, 0, 0, 1,
-                                             ctypes.byref(ci), ctypes.byref(mi), None, None))
+                                             ctypes.byref(pc), ctypes.byref(uc),
+                                             ctypes.byref(mi), None, None))
         chosen.append(mi.value - 1)
-    tm = T[okm_rows, N_CFG:N_CFG + N_METH]
+    tm = T[okm_rows, METH:METH + N_METH]
     best = tm.min(1)
     return regret(tm[np.arange(len(tm)), np.array(chosen)], best), chosen
 
@@ -340,11 +379,11 @@ def main(argv=None):
     ho = slice(n - h, n)
     report, _ = evaluate(params, args.members, y_mean, y_std, X[ho], T[ho], meta[ho])
     # the table model on the same held-out method rows
-    tabs, pp_dev, pp_host = measure_tables()
+    tabs, pp_dev, pp_host, d2h, h2d = measure_tables()
     tpath = os.path.join(out, TABLE_FILE)
-    write_tables(tpath, tabs, pp_dev, pp_host)
+    write_tables(tpath, tabs, pp_dev, pp_host, d2h, h2d)
     _lib.check(_lib.tempi().tempi_dispatch_load(None, tpath.encode()))
-    okm = np.isfinite(T[ho, N_CFG:N_CFG + N_METH]).all(1)
+    okm = np.isfinite(T[ho, METH:METH + N_METH]).all(1)
     if okm.any():
         ho_descs = [descs[n - h + i] for i in np.nonzero(okm)[0]]
         report["methods"]["table_model"], _ = table_regret(ho_descs, T[ho], okm)
@@ -354,10 +393,10 @@ def main(argv=None):
     if not args.no_install:
         os.makedirs(MODELS, exist_ok=True)
         write_model(os.path.join(MODELS, MODEL_FILE), params_np, args.members, y_mean, y_std, gpu)
-        write_tables(os.path.join(MODELS, TABLE_FILE), tabs, pp_dev, pp_host)
+        write_tables(os.path.join(MODELS, TABLE_FILE), tabs, pp_dev, pp_host, d2h, h2d)
     report.update({
         "gpu": gpu, "layouts_measured": n, "train_rows": n - h, "heldout_rows": h,
-        "method_rows": int(np.isfinite(T[:, N_CFG]).sum()),
+        "method_rows": int(np.isfinite(T[:, METH]).sum()),
         "measure_s": round(t_meas, 1), "train_s": round(t_train, 2), "epochs": epochs,
         "members": args.members, "loss_first_epoch": float(losses[:, 0].mean()),
         "loss_last_epoch": float(losses[:, -1].mean()),

@@ -13,7 +13,7 @@ from tempi_b200 import _lib
 def test_oracle_gradient_matches_finite_differences():
     rng = np.random.default_rng(0)
     p = M.init(1) + rng.normal(0, 0.01, M.P)
-    p[M.P - 11:] = rng.normal(0, 0.1, 11)  # non-zero output biases
+    p[M.P - M.OUT:] = rng.normal(0, 0.1, M.OUT)  # non-zero output biases
     x = rng.uniform(0, 1, (16, M.IN))
     y = rng.normal(0, 1, (16, M.OUT))
     mask = (rng.uniform(size=(16, M.OUT)) < 0.7).astype(float)
