@@ -1,15 +1,15 @@
-// The learned cost model's network: a 12 -> 64 -> 64 -> 11 FP32 perceptron
+// The learned cost model's network: a 12 -> 64 -> 64 -> 19 FP32 perceptron
 // with ReLU hidden layers, trained and run by these kernels.  It replaces the
 // reference's measured-parameter tables (src/internal/measure_system.cpp,
 // interp_2d :223-299) as the predictor of pack and transfer times.
 //
 // Layout of one member's parameters (floats, row-major [out][in]):
-//   W1[64][12] b1[64] W2[64][64] b2[64] W3[11][64] b3[11]   (5707 floats)
+//   W1[64][12] b1[64] W2[64][64] b2[64] W3[19][64] b3[19]   (6227 floats)
 // An ensemble is `members` such blocks back to back.
 //
 // Training: one CTA per member, the whole optimisation in one launch.  The
 // member's parameters, its gradient and its Adam moments live in shared
-// memory (4 x 5707 floats), as do the activations of one mini-batch, so
+// memory (4 x 6227 floats), as do the activations of one mini-batch, so
 // the only global traffic is the mini-batch rows.  Loss: squared error on
 // the observed outputs only (a mask marks them), averaged over them.
 
