@@ -763,13 +763,26 @@ def run_ours(args):
     top = max(table, key=lambda r: r["pack_ms"])
     peak, peak_kind = measured_peaks()
     achieved = top["pack_gbs"]
-    halo_res = halo_bench(torch, side) if rank == 0 else None
+    # the single-GPU characterisations run at N = 1 only: they would keep
+    # the other ranks waiting at the final barrier
+    solo = rank == 0 and world == 1
+    halo_res = halo_bench(torch, side) if solo else None
+    # end to end: every rank at once, the whole job's rate from the slowest
+    # rank's time (replicas: each rank moves its own copy of the workload)
+    barrier()
     e2e_staged = e2e_bench(torch, sw, mpi, max(1, args.steps // 2), 1)
+    barrier()
     e2e_zc = e2e_zero_copy(torch, sw, max(1, args.steps // 2), 1)
+    barrier()
+    for part in (e2e_staged, e2e_zc):
+        part["ms_per_step"] = round(reduce_max(part["ms_per_step"], dist, dev), 3)
+        part["value"] = round(world * sw.alg_bytes / part["ms_per_step"] / 1e6, 3)
+        part["h2d_bytes_per_step"] *= world
+        part["d2h_bytes_per_step"] *= world
     e2e = dict(e2e_zc, staged=e2e_staged)
-    send_res = sendrecv_bench(torch, mpi) if rank == 0 and not args.no_sendrecv else None
-    c1_res = config1_bench(torch, mpi) if rank == 0 else None
-    disp_res = dispatch_sample(torch) if rank == 0 and not args.no_sendrecv else None
+    send_res = sendrecv_bench(torch, mpi) if solo and not args.no_sendrecv else None
+    c1_res = config1_bench(torch, mpi) if solo else None
+    disp_res = dispatch_sample(torch) if solo and not args.no_sendrecv else None
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),

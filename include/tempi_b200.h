@@ -21,6 +21,9 @@
         MPI_Isend         replaces reference src/isend.cpp + src/internal/isend.cpp:15-45
         MPI_Irecv         replaces reference src/irecv.cpp + src/internal/irecv.cpp:15-44
         MPI_Wait          replaces reference src/wait.cpp:11-16
+        MPI_Neighbor_alltoallw
+                          replaces reference src/neighbor_alltoallw.cpp:11-17
+                          + src/internal/neighbor_alltoallw.cpp:19-85
 
       Signatures are those of include/symbols.hpp in the reference
       (PARAMS_MPI_* macros, lines 10-178).
@@ -124,6 +127,31 @@ int tempi_batch_launch(tempi_batch *b, void *stream);
 int tempi_batch_capture(tempi_batch *b, void *stream);
 int tempi_batch_replay(tempi_batch *b, void *stream);
 int tempi_batch_destroy(tempi_batch *b);
+
+/* Batched exchange: every region is copied from one strided layout straight
+   into another (typed -> typed, no packed buffer between them), all regions
+   in one launch, through the same batch handle (launch / capture / replay /
+   destroy above).  The bytes of `src_count` objects of `src_desc` at
+   `src_origin`, in type-map order, go to the bytes of `dst_count` objects of
+   `dst_desc` at `dst_origin`, in type-map order; both must describe the same
+   number of bytes.  This is a pack, a transfer and an unpack fused into one
+   kernel: a halo exchange with a periodic neighbour that is the same rank
+   (each send region lands in the opposite ghost region), and the local part
+   of MPI_Neighbor_alltoallw.  Replaces the pack -> MPI_Neighbor_alltoallv ->
+   unpack sequence of the reference's bin/bench_halo_exchange.cpp:560-625
+   and the Isend/Irecv pairs of src/internal/neighbor_alltoallw.cpp:19-85
+   for edges that stay on this GPU. */
+typedef struct tempi_copy_region {
+  const void *src_origin;
+  void *dst_origin;
+  tempi_desc src_desc;
+  tempi_desc dst_desc;
+  int64_t src_count;
+  int64_t dst_count;
+} tempi_copy_region;
+
+int tempi_batch_create_copy(const tempi_copy_region *regions, int32_t n,
+                            tempi_batch **out);
 
 /* Batched pack (unpack != 0: unpack) of `n` regions in one launch on
    `stream`, allocating nothing.  No counterpart in the reference.  For

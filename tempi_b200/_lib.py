@@ -95,6 +95,19 @@ class Region(ctypes.Structure):
     ]
 
 
+class CopyRegion(ctypes.Structure):
+    """``tempi_copy_region``."""
+
+    _fields_ = [
+        ("src_origin", c_void_p),
+        ("dst_origin", c_void_p),
+        ("src_desc", Desc),
+        ("dst_desc", Desc),
+        ("src_count", c_int64),
+        ("dst_count", c_int64),
+    ]
+
+
 class Status(ctypes.Structure):
     """``MPI_Status`` of libminimpi's mpi.h."""
 
@@ -142,13 +155,21 @@ _MPI_SIGS = {
     "MPI_Irecv": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, P(c_int)]),
     "MPI_Wait": (c_int, [P(c_int), P(Status)]),
     "MPI_Get_count": (c_int, [P(Status), c_int, P(c_int)]),
+    "MPI_Dist_graph_create_adjacent": (c_int, [c_int, c_int, c_void_p, c_void_p, c_int, c_void_p,
+                                               c_void_p, c_int, c_int, P(c_int)]),
+    "MPI_Dist_graph_neighbors_count": (c_int, [c_int, P(c_int), P(c_int), P(c_int)]),
+    "MPI_Comm_free": (c_int, [P(c_int)]),
+    "MPI_Neighbor_alltoallv": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                       c_void_p, c_int, c_int]),
+    "MPI_Neighbor_alltoallw": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_void_p, c_void_p, c_int]),
 }
 
 # the interposed entry points libtempi_b200.so must export
 INTERPOSED = [
     "MPI_Init", "MPI_Init_thread", "MPI_Finalize", "MPI_Type_commit",
     "MPI_Type_free", "MPI_Pack", "MPI_Unpack", "MPI_Send", "MPI_Recv",
-    "MPI_Isend", "MPI_Irecv", "MPI_Wait",
+    "MPI_Isend", "MPI_Irecv", "MPI_Wait", "MPI_Neighbor_alltoallw",
 ]
 
 _TEMPI_SIGS = {
@@ -161,6 +182,7 @@ _TEMPI_SIGS = {
     "tempi_batch_replay": (c_int, [c_void_p, c_void_p]),
     "tempi_batch_destroy": (c_int, [c_void_p]),
     "tempi_batch_run_static": (c_int, [P(Region), ctypes.c_int32, ctypes.c_int32, c_void_p]),
+    "tempi_batch_create_copy": (c_int, [P(CopyRegion), ctypes.c_int32, P(c_void_p)]),
     "tempi_last_error": (ctypes.c_char_p, []),
     "tempi_kernel_launches": (c_int64, []),
     "tempi_last_kernel": (ctypes.c_char_p, []),

@@ -385,7 +385,21 @@ std::deque<int> g_posted; // active receive requests, in posting order
 std::unordered_map<int, Req> g_reqs;
 int g_next_req = 1;
 
-bool valid_comm(MPI_Comm c) { return c == MPI_COMM_WORLD || c == MPI_COMM_SELF; }
+// Distributed graph communicators.  Point-to-point traffic of a
+// neighbourhood collective travels on the communicator's collective context
+// (the handle with kCollBit set), so it never matches user messages.
+struct Graph {
+  std::vector<int> sources, sweights, dests, dweights;
+  bool weighted = false;
+};
+std::unordered_map<MPI_Comm, Graph> g_graphs;
+MPI_Comm g_next_comm = 16;
+constexpr MPI_Comm kCollBit = 0x40000000;
+
+bool valid_comm(MPI_Comm c) {
+  c &= ~kCollBit;
+  return c == MPI_COMM_WORLD || c == MPI_COMM_SELF || g_graphs.count(c) > 0;
+}
 
 bool tag_match(int want, int have) { return want == MPI_ANY_TAG || want == have; }
 
@@ -1224,6 +1238,177 @@ int MPI_Waitall(int count, MPI_Request reqs[], MPI_Status stats[]) {
       err = e;
   }
   return err;
+}
+
+// ---- distributed graph topologies ---------------------------------------------
+
+int MPI_Dist_graph_create_adjacent(MPI_Comm comm_old, int indegree,
+                                   const int sources[],
+                                   const int sourceweights[], int outdegree,
+                                   const int destinations[],
+                                   const int destweights[], MPI_Info info,
+                                   int reorder, MPI_Comm *comm_dist_graph) {
+  (void)info;
+  (void)reorder; // one rank: nothing to reorder
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!valid_comm(comm_old) || (comm_old & kCollBit))
+    return MPI_ERR_COMM;
+  if (indegree < 0 || outdegree < 0 || !comm_dist_graph ||
+      (indegree > 0 && !sources) || (outdegree > 0 && !destinations))
+    return MPI_ERR_ARG;
+  Graph g;
+  g.weighted = sourceweights != MPI_UNWEIGHTED && destweights != MPI_UNWEIGHTED;
+  for (int i = 0; i < indegree; ++i) {
+    if (sources[i] != 0)
+      return MPI_ERR_RANK;
+    g.sources.push_back(0);
+    g.sweights.push_back(g.weighted && sourceweights != MPI_WEIGHTS_EMPTY
+                             ? sourceweights[i]
+                             : 1);
+  }
+  for (int i = 0; i < outdegree; ++i) {
+    if (destinations[i] != 0)
+      return MPI_ERR_RANK;
+    g.dests.push_back(0);
+    g.dweights.push_back(g.weighted && destweights != MPI_WEIGHTS_EMPTY
+                             ? destweights[i]
+                             : 1);
+  }
+  const MPI_Comm c = g_next_comm++;
+  g_graphs[c] = std::move(g);
+  *comm_dist_graph = c;
+  return MPI_SUCCESS;
+}
+
+int MPI_Dist_graph_neighbors_count(MPI_Comm comm, int *indegree,
+                                   int *outdegree, int *weighted) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  auto it = g_graphs.find(comm);
+  if (it == g_graphs.end())
+    return MPI_ERR_COMM;
+  if (indegree)
+    *indegree = int(it->second.sources.size());
+  if (outdegree)
+    *outdegree = int(it->second.dests.size());
+  if (weighted)
+    *weighted = it->second.weighted ? 1 : 0;
+  return MPI_SUCCESS;
+}
+
+int MPI_Dist_graph_neighbors(MPI_Comm comm, int maxindegree, int sources[],
+                             int sourceweights[], int maxoutdegree,
+                             int destinations[], int destweights[]) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  auto it = g_graphs.find(comm);
+  if (it == g_graphs.end())
+    return MPI_ERR_COMM;
+  const Graph &g = it->second;
+  for (int i = 0; i < maxindegree && i < int(g.sources.size()); ++i) {
+    sources[i] = g.sources[i];
+    if (g.weighted && sourceweights && sourceweights != MPI_UNWEIGHTED)
+      sourceweights[i] = g.sweights[i];
+  }
+  for (int i = 0; i < maxoutdegree && i < int(g.dests.size()); ++i) {
+    destinations[i] = g.dests[i];
+    if (g.weighted && destweights && destweights != MPI_UNWEIGHTED)
+      destweights[i] = g.dweights[i];
+  }
+  return MPI_SUCCESS;
+}
+
+int MPI_Comm_free(MPI_Comm *comm) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!comm || !g_graphs.count(*comm))
+    return MPI_ERR_COMM;
+  g_graphs.erase(*comm);
+  *comm = MPI_COMM_NULL;
+  return MPI_SUCCESS;
+}
+
+extern "C++" {
+namespace {
+
+// Post every receive, then every send, on the collective context, and wait
+// for all: with FIFO matching per (source, tag) the k-th edge to rank 0 meets
+// the k-th edge from it, as MPI-3.1 7.6 requires for repeated edges.
+template <typename SendAt, typename RecvAt>
+int neighbor_exchange(MPI_Comm comm, SendAt send_at, RecvAt recv_at) {
+  auto it = g_graphs.find(comm);
+  if (it == g_graphs.end())
+    return MPI_ERR_COMM;
+  const Graph &g = it->second;
+  const MPI_Comm cc = comm | kCollBit;
+  std::vector<MPI_Request> reqs;
+  int err = MPI_SUCCESS;
+  for (size_t j = 0; j < g.sources.size() && !err; ++j) {
+    void *buf;
+    int count;
+    MPI_Datatype t;
+    recv_at(j, &buf, &count, &t);
+    MPI_Request r;
+    err = MPI_Irecv(buf, count, t, g.sources[j], 0, cc, &r);
+    if (!err)
+      reqs.push_back(r);
+  }
+  for (size_t i = 0; i < g.dests.size() && !err; ++i) {
+    const void *buf;
+    int count;
+    MPI_Datatype t;
+    send_at(i, &buf, &count, &t);
+    MPI_Request r;
+    err = MPI_Isend(buf, count, t, g.dests[i], 0, cc, &r);
+    if (!err)
+      reqs.push_back(r);
+  }
+  const int werr = MPI_Waitall(int(reqs.size()), reqs.data(), MPI_STATUSES_IGNORE);
+  return err ? err : werr;
+}
+
+} // namespace
+} // extern "C++"
+
+int MPI_Neighbor_alltoallv(const void *sendbuf, const int sendcounts[],
+                           const int sdispls[], MPI_Datatype sendtype,
+                           void *recvbuf, const int recvcounts[],
+                           const int rdispls[], MPI_Datatype recvtype,
+                           MPI_Comm comm) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  const TypeRec *st = get(sendtype), *rt = get(recvtype);
+  if (!st || !rt)
+    return MPI_ERR_TYPE;
+  const int64_t se = st->extent(), re = rt->extent();
+  return neighbor_exchange(
+      comm,
+      [&](size_t i, const void **b, int *n, MPI_Datatype *t) {
+        *b = (const char *)sendbuf + int64_t(sdispls[i]) * se;
+        *n = sendcounts[i];
+        *t = sendtype;
+      },
+      [&](size_t j, void **b, int *n, MPI_Datatype *t) {
+        *b = (char *)recvbuf + int64_t(rdispls[j]) * re;
+        *n = recvcounts[j];
+        *t = recvtype;
+      });
+}
+
+int MPI_Neighbor_alltoallw(const void *sendbuf, const int sendcounts[],
+                           const MPI_Aint sdispls[],
+                           const MPI_Datatype sendtypes[], void *recvbuf,
+                           const int recvcounts[], const MPI_Aint rdispls[],
+                           const MPI_Datatype recvtypes[], MPI_Comm comm) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  return neighbor_exchange(
+      comm,
+      [&](size_t i, const void **b, int *n, MPI_Datatype *t) {
+        *b = (const char *)sendbuf + sdispls[i];
+        *n = sendcounts[i];
+        *t = sendtypes[i];
+      },
+      [&](size_t j, void **b, int *n, MPI_Datatype *t) {
+        *b = (char *)recvbuf + rdispls[j];
+        *n = recvcounts[j];
+        *t = recvtypes[j];
+      });
 }
 
 int MPI_Request_free(MPI_Request *request) {

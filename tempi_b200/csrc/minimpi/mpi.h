@@ -25,6 +25,7 @@ typedef int MPI_Datatype;
 typedef int MPI_Comm;
 typedef int MPI_Request;
 typedef int MPI_Op;
+typedef int MPI_Info;
 typedef intptr_t MPI_Aint;
 typedef long long MPI_Count;
 
@@ -111,6 +112,11 @@ typedef struct MPI_Status {
 #define MPI_THREAD_MULTIPLE 3
 
 #define MPI_MAX_LIBRARY_VERSION_STRING 256
+
+/* distributed graph topologies */
+#define MPI_INFO_NULL 0
+#define MPI_UNWEIGHTED ((int *)1)
+#define MPI_WEIGHTS_EMPTY ((int *)2)
 
 /* environment */
 int MPI_Init(int *argc, char ***argv);
@@ -199,6 +205,33 @@ int MPI_Waitall(int count, MPI_Request array_of_requests[],
                 MPI_Status array_of_statuses[]);
 int MPI_Request_free(MPI_Request *request);
 int MPI_Get_count(const MPI_Status *status, MPI_Datatype datatype, int *count);
+
+/* distributed graph communicators (MPI-3.1 7.5.4) and neighbourhood
+   collectives (7.6).  In a world of one rank every neighbour is rank 0;
+   the k-th edge to a neighbour is matched with the k-th edge from it, in
+   the order the neighbour lists give. */
+int MPI_Dist_graph_create_adjacent(MPI_Comm comm_old, int indegree,
+                                   const int sources[],
+                                   const int sourceweights[], int outdegree,
+                                   const int destinations[],
+                                   const int destweights[], MPI_Info info,
+                                   int reorder, MPI_Comm *comm_dist_graph);
+int MPI_Dist_graph_neighbors_count(MPI_Comm comm, int *indegree,
+                                   int *outdegree, int *weighted);
+int MPI_Dist_graph_neighbors(MPI_Comm comm, int maxindegree, int sources[],
+                             int sourceweights[], int maxoutdegree,
+                             int destinations[], int destweights[]);
+int MPI_Comm_free(MPI_Comm *comm);
+int MPI_Neighbor_alltoallv(const void *sendbuf, const int sendcounts[],
+                           const int sdispls[], MPI_Datatype sendtype,
+                           void *recvbuf, const int recvcounts[],
+                           const int rdispls[], MPI_Datatype recvtype,
+                           MPI_Comm comm);
+int MPI_Neighbor_alltoallw(const void *sendbuf, const int sendcounts[],
+                           const MPI_Aint sdispls[],
+                           const MPI_Datatype sendtypes[], void *recvbuf,
+                           const int recvcounts[], const MPI_Aint rdispls[],
+                           const MPI_Datatype recvtypes[], MPI_Comm comm);
 
 #ifdef __cplusplus
 }

@@ -13,6 +13,13 @@
 // A batch can capture one launch into a CUDA graph and replay it; because
 // the pointers live in the table, replays see new buffer contents without
 // re-capture.
+//
+// A copy batch (tempi_batch_create_copy) fuses pack, transfer and unpack:
+// each entry pairs a source layout with a destination layout of the same
+// byte count, and word w of the entry is read at the source geometry's
+// offset of w and written at the destination geometry's offset of w.  Both
+// geometries are built at the same proven width, so one word index walks
+// both.
 
 #include "internal.hpp"
 
@@ -107,9 +114,9 @@ __device__ __forceinline__ void copy_chunk(const BatchRegion &r, uint32_t w0,
 // stretch with one coalesced load and a ballot narrows it 32-fold, so n
 // regions take ceil(log32 n) dependent loads (one for a 26-region halo, two
 // for up to 1024 regions) instead of a binary search's log2 n.
-__device__ __forceinline__ int find_region(const BatchRegion *__restrict__ r,
-                                           int n, uint32_t chunk,
-                                           uint32_t lane) {
+template <typename Rec>
+__device__ __forceinline__ int find_region(const Rec *__restrict__ r, int n,
+                                           uint32_t chunk, uint32_t lane) {
   int base = 0, len = n;
   while (true) {
     const int step = (len + 31) / 32;
@@ -160,11 +167,89 @@ __global__ void __launch_bounds__(kBatchThreads, 3)
   }
 }
 
+struct CopyPair {
+  const char *src; // src origin + start
+  char *dst;       // dst origin + start
+  Geometry gs, gd; // same width and word count
+  uint32_t chunk_begin;
+  uint32_t pad;
+};
+
+template <int W>
+__device__ __forceinline__ void copy_pair_chunk(const CopyPair &r, uint32_t w0) {
+  using T = typename std::conditional<
+      W == 16, uint4,
+      typename std::conditional<
+          W == 8, uint2,
+          typename std::conditional<
+              W == 4, uint32_t,
+              typename std::conditional<W == 2, uint16_t,
+                                        uint8_t>::type>::type>::type>::type;
+  const uint32_t total = r.gs.total_words;
+  // each load is issued as soon as its source offset is known; only the
+  // destination offsets and the loaded words stay live until the stores
+  int64_t dof[kBatchUnroll];
+  T v[kBatchUnroll];
+#pragma unroll
+  for (int u = 0; u < kBatchUnroll; ++u) {
+    const uint32_t ww = w0 + threadIdx.x + u * kBatchThreads;
+    if (ww < total) {
+      const uint32_t rs = bdiv(ww, r.gs.wdiv);
+      v[u] = __ldg(reinterpret_cast<const T *>(
+          r.src + brow_offset(rs, r.gs) + int64_t(ww - rs * r.gs.wpr) * W));
+      const uint32_t rd = bdiv(ww, r.gd.wdiv);
+      dof[u] = brow_offset(rd, r.gd) + int64_t(ww - rd * r.gd.wpr) * W;
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kBatchUnroll; ++u)
+    if (w0 + threadIdx.x + u * kBatchThreads < total)
+      *reinterpret_cast<T *>(r.dst + dof[u]) = v[u];
+}
+
+__global__ void __launch_bounds__(kBatchThreads, 2)
+    k_batch_copy(const CopyPair *__restrict__ pairs, int npairs,
+                 uint32_t total_chunks) {
+  __shared__ CopyPair sp;
+  __shared__ int cur;
+  const uint32_t lane = threadIdx.x & 31;
+  if (threadIdx.x == 0)
+    cur = -1;
+  __syncthreads();
+  for (uint32_t chunk = blockIdx.x; chunk < total_chunks; chunk += gridDim.x) {
+    if (threadIdx.x < 32) {
+      const int idx = find_region(pairs, npairs, chunk, lane);
+      if (idx != cur) {
+        constexpr int kWords = sizeof(CopyPair) / 4;
+        const uint32_t *from = reinterpret_cast<const uint32_t *>(pairs + idx);
+        uint32_t *to = reinterpret_cast<uint32_t *>(&sp);
+        for (int w = lane; w < kWords; w += 32)
+          to[w] = from[w];
+        __syncwarp();
+        if (lane == 0)
+          cur = idx;
+      }
+    }
+    __syncthreads();
+    const uint32_t w0 = (chunk - sp.chunk_begin) * kChunkWords;
+    switch (sp.gs.width) {
+    case 16: copy_pair_chunk<16>(sp, w0); break;
+    case 8: copy_pair_chunk<8>(sp, w0); break;
+    case 4: copy_pair_chunk<4>(sp, w0); break;
+    case 2: copy_pair_chunk<2>(sp, w0); break;
+    default: copy_pair_chunk<1>(sp, w0); break;
+    }
+    __syncthreads();
+  }
+}
+
 } // namespace
 
 struct BatchImpl {
   std::vector<BatchRegion> host;
   BatchRegion *dev = nullptr;
+  std::vector<CopyPair> host_pairs; // a copy batch
+  CopyPair *dev_pairs = nullptr;
   uint32_t total_chunks = 0;
   int unpack = 0;
   cudaGraph_t graph = nullptr;
@@ -229,6 +314,18 @@ extern "C" int tempi_batch_create(const tempi_region *regions, int32_t n,
 
 static int batch_launch(tempi_batch *b, cudaStream_t s) {
   BatchImpl &bi = b->impl;
+  if (!bi.host_pairs.empty()) {
+    const uint32_t grid = std::max<uint32_t>(
+        1, std::min<uint32_t>(bi.total_chunks, num_sms() * 8));
+    k_batch_copy<<<grid, kBatchThreads, 0, s>>>(
+        bi.dev_pairs, int(bi.host_pairs.size()), bi.total_chunks);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+      return cuda_error(e, "copy batch launch");
+    counters().kernel_launches++;
+    set_last_kernel("batch_copy");
+    return TEMPI_OK;
+  }
   if (bi.host.empty())
     return TEMPI_OK;
   const int sms = num_sms();
@@ -243,6 +340,128 @@ static int batch_launch(tempi_batch *b, cudaStream_t s) {
   set_last_kernel(bi.unpack ? "batch_unpack" : "batch_pack");
   return TEMPI_OK;
 }
+
+// Copy pairs for `regions`; empty regions are dropped.  Returns the chunk
+// count through *chunks_out.
+static int build_pairs(const tempi_copy_region *regions, int32_t n,
+                       std::vector<CopyPair> *pairs, uint32_t *chunks_out) {
+  uint64_t chunks = 0;
+  pairs->clear();
+  for (int32_t i = 0; i < n; ++i) {
+    const tempi_copy_region &r = regions[i];
+    if (r.src_count < 0 || r.dst_count < 0 ||
+        r.src_desc.size * r.src_count != r.dst_desc.size * r.dst_count) {
+      return set_error(TEMPI_ERR_ARG,
+                       "copy region %d: source and destination sizes differ",
+                       int(i));
+    }
+    const char *src = (const char *)r.src_origin + r.src_desc.start;
+    char *dst = (char *)r.dst_origin + r.dst_desc.start;
+    CopyPair cp{};
+    bool es = false, ed = false;
+    // the widest width both layouts prove, then both geometries at it
+    int err = make_geometry(&r.src_desc, r.src_count, uintptr_t(src), 0, 0,
+                            &cp.gs, &es);
+    if (!err)
+      err = make_geometry(&r.dst_desc, r.dst_count, uintptr_t(dst), 0, 0,
+                          &cp.gd, &ed);
+    if (!err && !es && !ed) {
+      const int w = int(std::min(cp.gs.width, cp.gd.width));
+      err = make_geometry(&r.src_desc, r.src_count, uintptr_t(src), 0, w,
+                          &cp.gs, &es);
+      if (!err)
+        err = make_geometry(&r.dst_desc, r.dst_count, uintptr_t(dst), 0, w,
+                            &cp.gd, &ed);
+    }
+    if (err)
+      return err;
+    if (es || ed)
+      continue; // nothing to copy
+    if (cp.gs.width != cp.gd.width || cp.gs.total_words != cp.gd.total_words)
+      return set_error(TEMPI_ERR_ARG, "copy region %d: layouts disagree",
+                       int(i));
+    cp.src = src;
+    cp.dst = dst;
+    cp.chunk_begin = uint32_t(chunks);
+    chunks += (cp.gs.total_words + kChunkWords - 1) / kChunkWords;
+    if (chunks > UINT32_MAX)
+      return set_error(TEMPI_ERR_ARG, "batch too large");
+    pairs->push_back(cp);
+  }
+  *chunks_out = uint32_t(chunks);
+  return TEMPI_OK;
+}
+
+extern "C" int tempi_batch_create_copy(const tempi_copy_region *regions,
+                                       int32_t n, tempi_batch **out) {
+  if (!out || n < 0 || (n > 0 && !regions))
+    return set_error(TEMPI_ERR_ARG, "bad copy batch arguments");
+  *out = nullptr;
+  auto *b = new tempi_batch();
+  int err = build_pairs(regions, n, &b->impl.host_pairs, &b->impl.total_chunks);
+  if (err) {
+    delete b;
+    return err;
+  }
+  if (!b->impl.host_pairs.empty()) {
+    const size_t bytes = b->impl.host_pairs.size() * sizeof(CopyPair);
+    cudaError_t e = cudaMalloc(&b->impl.dev_pairs, bytes);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(b->impl.dev_pairs, b->impl.host_pairs.data(), bytes,
+                     cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cudaFree(b->impl.dev_pairs);
+      delete b;
+      return cuda_error(e, "copy batch table upload");
+    }
+  }
+  *out = b;
+  return TEMPI_OK;
+}
+
+namespace tempi {
+
+// One copy batch on `s` with the pair table in a grow-only device buffer:
+// no allocation once the buffer is large enough.  The caller synchronises
+// `s` before the next call (the table is rewritten by every call).
+int copy_batch_run(const tempi_copy_region *regions, int32_t n,
+                   cudaStream_t s) {
+  static std::mutex mu;
+  static CopyPair *table = nullptr;
+  static size_t capacity = 0;
+  static std::vector<CopyPair> pairs;
+  std::lock_guard<std::mutex> l(mu);
+  uint32_t chunks = 0;
+  int err = build_pairs(regions, n, &pairs, &chunks);
+  if (err || pairs.empty())
+    return err;
+  if (pairs.size() > capacity) {
+    cudaFree(table);
+    table = nullptr;
+    capacity = 0;
+    const size_t want = std::max<size_t>(pairs.size(), 64);
+    cudaError_t e = cudaMalloc(&table, want * sizeof(CopyPair));
+    if (e != cudaSuccess)
+      return cuda_error(e, "copy table allocation");
+    capacity = want;
+  }
+  cudaError_t e = cudaMemcpyAsync(table, pairs.data(),
+                                  pairs.size() * sizeof(CopyPair),
+                                  cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess)
+    return cuda_error(e, "copy table upload");
+  const uint32_t grid =
+      std::max<uint32_t>(1, std::min<uint32_t>(chunks, num_sms() * 8));
+  k_batch_copy<<<grid, kBatchThreads, 0, s>>>(table, int(pairs.size()), chunks);
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return cuda_error(e, "copy batch launch");
+  counters().kernel_launches++;
+  set_last_kernel("batch_copy");
+  return TEMPI_OK;
+}
+
+} // namespace tempi
 
 extern "C" int tempi_batch_launch(tempi_batch *b, void *stream) {
   if (!b)
@@ -282,7 +501,7 @@ extern "C" int tempi_batch_replay(tempi_batch *b, void *stream) {
   cudaError_t e = cudaGraphLaunch(b->impl.exec, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess)
     return cuda_error(e, "graph launch");
-  if (!b->impl.host.empty())
+  if (!b->impl.host.empty() || !b->impl.host_pairs.empty())
     counters().kernel_launches++;
   return TEMPI_OK;
 }
@@ -414,6 +633,7 @@ extern "C" int tempi_batch_destroy(tempi_batch *b) {
   if (b->impl.graph)
     cudaGraphDestroy(b->impl.graph);
   cudaFree(b->impl.dev);
+  cudaFree(b->impl.dev_pairs);
   delete b;
   return TEMPI_OK;
 }

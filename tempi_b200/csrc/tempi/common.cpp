@@ -65,7 +65,8 @@ extern "C" int64_t tempi_counter(const char *name) {
   C(send_staged) C(send_lib) C(recv_device) C(recv_oneshot) C(recv_staged)
   C(recv_lib) C(isend_managed) C(irecv_managed) C(dispatch_hit)
   C(dispatch_miss) C(slab_hits) C(slab_misses) C(slab_bytes) C(host_link_copies)
-  C(send_contig_staged) C(recv_contig_staged)
+  C(send_contig_staged) C(recv_contig_staged) C(neighbor_fused)
+  C(neighbor_isir) C(neighbor_lib)
 #undef C
   return -1;
 }

@@ -49,6 +49,7 @@ struct Counters {
   std::atomic<int64_t> cached_types{0};
   std::atomic<int64_t> host_link_copies{0};
   std::atomic<int64_t> send_contig_staged{0}, recv_contig_staged{0};
+  std::atomic<int64_t> neighbor_fused{0}, neighbor_isir{0}, neighbor_lib{0};
 };
 Counters &counters();
 
@@ -107,5 +108,11 @@ int launch_geometry(const Geometry &g, const char *strided_base, char *packed,
                     bool unpack, const tempi_config *cfg, cudaStream_t stream);
 
 int num_sms();
+
+// The copy batch's kernel (tempi_batch_create_copy) for one call, with its
+// pair table in a grow-only device buffer; launches on `s`, which the caller
+// synchronises before calling again.
+int copy_batch_run(const tempi_copy_region *regions, int32_t n,
+                   cudaStream_t s);
 
 } // namespace tempi

@@ -18,6 +18,8 @@
 #include "runtime.hpp"
 #include "sender.hpp"
 
+#include <vector>
+
 namespace tempi {
 namespace {
 
@@ -37,7 +39,7 @@ int to_mpi(int e) {
 // copy engines move it across the host link (hostlink.cpp).
 bool use_host_link(const PtrInfo &a, const PtrInfo &b, const tempi_desc &d,
                    int64_t count) {
-  if (!env().host_link_dma || a.is_device || b.is_device)
+  if (!env().host_link_dma || !a.is_host || !b.is_host)
     return false;
   if (int64_t(count) * d.size < kHostLinkMinBytes)
     return false;
@@ -158,7 +160,7 @@ int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
                        size_t(bytes), s);
   } else {
     tempi_config cfg =
-        choose_config(*r, incount, !in.is_device, !out.is_device, false);
+        choose_config(*r, incount, in.is_host, out.is_host, false);
     e = tempi_pack(&r->desc, in.device_ptr, incount,
                    static_cast<char *>(out.device_ptr) + *position, &cfg, s);
   }
@@ -205,7 +207,7 @@ int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
                        size_t(bytes), s);
   } else {
     tempi_config cfg =
-        choose_config(*r, outcount, !out.is_device, !in.is_device, true);
+        choose_config(*r, outcount, out.is_host, in.is_host, true);
     e = tempi_unpack(&r->desc,
                      static_cast<const char *>(in.device_ptr) + *position,
                      outcount, out.device_ptr, &cfg, s);
@@ -298,6 +300,109 @@ int MPI_Irecv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
     err = libmpi.Irecv(buf, count, datatype, source, tag, comm, request);
   }
   try_progress();
+  return err;
+}
+
+// Neighbourhood all-to-all with a datatype per edge (reference
+// src/neighbor_alltoallw.cpp:11-17 -> neighbor_alltoallw::isir,
+// src/internal/neighbor_alltoallw.cpp:19-85: an MPI_Isend per out-edge and
+// an MPI_Irecv per in-edge, then waits).  When every edge is an edge to this
+// rank and every region is a committed strided type in device-accessible
+// memory, the k-th out-edge's region is copied straight into the k-th
+// in-edge's region by one fused kernel (copy_batch_run): pack, transfer and
+// unpack in one launch, no packed buffer.  Otherwise the reference's
+// Isend/Irecv sequence runs through TEMPI's own senders, and calls with no
+// region TEMPI can describe go to the library.
+int MPI_Neighbor_alltoallw(const void *sendbuf, const int sendcounts[],
+                           const MPI_Aint sdispls[],
+                           const MPI_Datatype sendtypes[], void *recvbuf,
+                           const int recvcounts[], const MPI_Aint rdispls[],
+                           const MPI_Datatype recvtypes[], MPI_Comm comm) {
+  if (!ready())
+    return MPI_ERR_OTHER;
+  if (env().disable)
+    return libmpi.Neighbor_alltoallw(sendbuf, sendcounts, sdispls, sendtypes,
+                                     recvbuf, recvcounts, rdispls, recvtypes,
+                                     comm);
+  int indeg = 0, outdeg = 0, weighted = 0, me = 0;
+  int err = libmpi.Dist_graph_neighbors_count(comm, &indeg, &outdeg, &weighted);
+  if (err)
+    return err;
+  std::vector<int> sources(size_t(indeg) + 1), sw(size_t(indeg) + 1);
+  std::vector<int> dests(size_t(outdeg) + 1), dw(size_t(outdeg) + 1);
+  err = libmpi.Dist_graph_neighbors(comm, indeg, sources.data(), sw.data(),
+                                    outdeg, dests.data(), dw.data());
+  if (!err)
+    err = libmpi.Comm_rank(comm, &me);
+  if (err)
+    return err;
+  const PtrInfo ps = classify(sendbuf), pr = classify(recvbuf);
+  bool any_described = false, fusable = indeg == outdeg && ps.device_accessible &&
+                                        pr.device_accessible;
+  std::vector<tempi_copy_region> regs;
+  for (int k = 0; k < outdeg; ++k) {
+    const TypeRecord *ts = find_type(sendtypes[k]);
+    const TypeRecord *tr = k < indeg ? find_type(recvtypes[k]) : nullptr;
+    const bool ds = ts && ts->packable, dr = tr && tr->packable;
+    any_described = any_described || ds || dr;
+    if (!fusable)
+      continue;
+    if (dests[k] != me || sources[k] != me || !ds || !dr ||
+        sendcounts[k] < 0 || recvcounts[k] < 0 ||
+        int64_t(sendcounts[k]) * ts->desc.size !=
+            int64_t(recvcounts[k]) * tr->desc.size) {
+      fusable = false;
+      continue;
+    }
+    tempi_copy_region c{};
+    c.src_origin = static_cast<const char *>(ps.device_ptr) + sdispls[k];
+    c.dst_origin = static_cast<char *>(pr.device_ptr) + rdispls[k];
+    c.src_desc = ts->desc;
+    c.dst_desc = tr->desc;
+    c.src_count = sendcounts[k];
+    c.dst_count = recvcounts[k];
+    regs.push_back(c);
+  }
+  if (fusable) {
+    cudaStream_t s = pack_stream();
+    int e = copy_batch_run(regs.data(), int32_t(regs.size()), s);
+    if (!e) {
+      cudaError_t ce = cudaStreamSynchronize(s);
+      if (ce != cudaSuccess)
+        e = cuda_error(ce, "MPI_Neighbor_alltoallw synchronize");
+    }
+    counters().neighbor_fused++;
+    return to_mpi(e);
+  }
+  if (!any_described) {
+    counters().neighbor_lib++;
+    return libmpi.Neighbor_alltoallw(sendbuf, sendcounts, sdispls, sendtypes,
+                                     recvbuf, recvcounts, rdispls, recvtypes,
+                                     comm);
+  }
+  counters().neighbor_isir++;
+  const int tag = 0x7ee1; // reserved for this collective
+  std::vector<MPI_Request> sreqs, rreqs;
+  for (int i = 0; i < outdeg && !err; ++i) {
+    MPI_Request q = MPI_REQUEST_NULL;
+    err = MPI_Isend(static_cast<const char *>(sendbuf) + sdispls[i],
+                    sendcounts[i], sendtypes[i], dests[i], tag, comm, &q);
+    sreqs.push_back(q);
+  }
+  for (int j = 0; j < indeg && !err; ++j) {
+    MPI_Request q = MPI_REQUEST_NULL;
+    err = MPI_Irecv(static_cast<char *>(recvbuf) + rdispls[j], recvcounts[j],
+                    recvtypes[j], sources[j], tag, comm, &q);
+    rreqs.push_back(q);
+  }
+  for (MPI_Request &q : sreqs) {
+    const int e = q == MPI_REQUEST_NULL ? MPI_SUCCESS : MPI_Wait(&q, MPI_STATUS_IGNORE);
+    err = err ? err : e;
+  }
+  for (MPI_Request &q : rreqs) {
+    const int e = q == MPI_REQUEST_NULL ? MPI_SUCCESS : MPI_Wait(&q, MPI_STATUS_IGNORE);
+    err = err ? err : e;
+  }
   return err;
 }
 

@@ -120,6 +120,7 @@ PtrInfo classify(const void *p) {
   }
   info.device_accessible = a.devicePointer != nullptr;
   info.is_device = a.type == cudaMemoryTypeDevice;
+  info.is_host = a.type == cudaMemoryTypeHost;
   info.device_ptr = a.devicePointer;
   return info;
 }

@@ -68,6 +68,7 @@ bool cuda_available();
 struct PtrInfo {
   bool device_accessible = false; // device memory, managed, or mapped host
   bool is_device = false;         // device memory proper
+  bool is_host = false;           // pinned host memory (not managed)
   void *device_ptr = nullptr;
 };
 PtrInfo classify(const void *p);

@@ -78,6 +78,9 @@ bool resolve_symbols() {
     LOAD(Type_contiguous);
     LOAD(Type_create_hvector);
     LOAD(Type_create_resized);
+    LOAD(Dist_graph_neighbors_count);
+    LOAD(Dist_graph_neighbors);
+    LOAD(Neighbor_alltoallw);
 #undef LOAD
     ok = r;
   });

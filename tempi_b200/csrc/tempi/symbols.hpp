@@ -44,6 +44,11 @@ struct LibMPI {
   int (*Type_contiguous)(int, MPI_Datatype, MPI_Datatype *);
   int (*Type_create_hvector)(int, int, MPI_Aint, MPI_Datatype, MPI_Datatype *);
   int (*Type_create_resized)(MPI_Datatype, MPI_Aint, MPI_Aint, MPI_Datatype *);
+  int (*Dist_graph_neighbors_count)(MPI_Comm, int *, int *, int *);
+  int (*Dist_graph_neighbors)(MPI_Comm, int, int[], int[], int, int[], int[]);
+  int (*Neighbor_alltoallw)(const void *, const int[], const MPI_Aint[],
+                            const MPI_Datatype[], void *, const int[],
+                            const MPI_Aint[], const MPI_Datatype[], MPI_Comm);
 };
 
 // Resolve the table once; returns false (and logs) if any symbol is missing.

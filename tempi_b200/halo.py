@@ -12,6 +12,16 @@ reference's halo benchmark (bin/bench_halo_exchange.cpp).
 launch through tempi_batch_* (and can replay it from a CUDA graph);
 ``pack_plain`` does the same with one MPI_Pack call per region, the
 reference's per-call path.
+
+A grid whose neighbours in every direction are the grid itself (one rank,
+periodic boundaries, as the reference's halo benchmark runs at world size 1)
+exchanges its halo by copying each send region into the ghost region on the
+opposite side.  ``HaloExchange`` does that with the fused copy kernel
+(tempi_batch_create_copy: no packed buffer, one launch); ``exchange_alltoallw``
+does it through the interposed MPI_Neighbor_alltoallw over a graph
+communicator with 26 self-edges; ``exchange_plain`` is the reference's
+sequence (26 MPI_Pack, MPI_Neighbor_alltoallv of the packed bytes, 26
+MPI_Unpack; bin/bench_halo_exchange.cpp:560-625).
 """
 from __future__ import annotations
 
@@ -122,6 +132,82 @@ class HaloBatch:
             self.close()
         except Exception:
             pass
+
+
+def copy_regions(grids, grid_ptrs):
+    """tempi_copy_region entries for a periodic self-exchange of every grid:
+    the send region of direction d goes to the ghost region of -d."""
+    out = []
+    for g, gp in zip(grids, grid_ptrs):
+        for d in directions():
+            err, sd = mpi.describe(g.send[d])
+            _lib.check(err, "tempi_describe")
+            err, rd = mpi.describe(g.recv[tuple(-x for x in d)])
+            _lib.check(err, "tempi_describe")
+            c = _lib.CopyRegion()
+            c.src_origin = gp
+            c.dst_origin = gp
+            c.src_desc = sd
+            c.dst_desc = rd
+            c.src_count = 1
+            c.dst_count = 1
+            out.append(c)
+    return out
+
+
+class HaloExchange(HaloBatch):
+    """The whole periodic self-exchange of `grids` in one fused launch; the
+    handle launches, captures, replays and closes like a HaloBatch."""
+
+    def __init__(self, grids, grid_ptrs):
+        regs = copy_regions(grids, grid_ptrs)
+        arr = (_lib.CopyRegion * len(regs))(*regs)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.tempi().tempi_batch_create_copy(arr, len(regs), ctypes.byref(h)),
+                   "tempi_batch_create_copy")
+        self.h = h
+        self.nregions = len(regs)
+
+
+class SelfGraph:
+    """A graph communicator with 26 self-edges (one per direction) and the
+    per-edge arguments of MPI_Neighbor_alltoallv / MPI_Neighbor_alltoallw for
+    one grid."""
+
+    def __init__(self, grid: Grid):
+        n = len(directions())
+        err, self.comm = mpi.Dist_graph_create_adjacent([0] * n, [0] * n)
+        _lib.check(err, "MPI_Dist_graph_create_adjacent")
+        self.grid = grid
+        offs = grid.offsets()
+        self.counts = [grid.region_bytes[d] for d in directions()]
+        self.displs = [offs[d] for d in directions()]
+        self.sendtypes = [grid.send[d] for d in directions()]
+        self.recvtypes = [grid.recv[tuple(-x for x in d)] for d in directions()]
+
+    def close(self):
+        if self.comm:
+            mpi.Comm_free(self.comm)
+            self.comm = 0
+
+
+def exchange_alltoallw(g: SelfGraph, grid_ptr: int) -> None:
+    n = len(g.sendtypes)
+    err = mpi.Neighbor_alltoallw(grid_ptr, [1] * n, [0] * n, g.sendtypes, grid_ptr,
+                                 [1] * n, [0] * n, g.recvtypes, g.comm)
+    if err:
+        raise RuntimeError(f"MPI_Neighbor_alltoallw failed: {err} {_lib.last_error()}")
+
+
+def exchange_plain(g: SelfGraph, grid_ptr: int, sendbuf: int, recvbuf: int) -> None:
+    """The reference's sequence: pack every region, exchange the packed bytes
+    with MPI_Neighbor_alltoallv, unpack every region."""
+    pack_plain(g.grid, grid_ptr, sendbuf)
+    err = mpi.Neighbor_alltoallv(sendbuf, g.counts, g.displs, mpi.BYTE, recvbuf, g.counts,
+                                 g.displs, mpi.BYTE, g.comm)
+    if err:
+        raise RuntimeError(f"MPI_Neighbor_alltoallv failed: {err}")
+    unpack_plain(g.grid, recvbuf, grid_ptr)
 
 
 def pack_plain(grid: Grid, grid_ptr: int, packed_ptr: int) -> int:

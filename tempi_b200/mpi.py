@@ -202,6 +202,56 @@ def Get_count(st, t: int) -> int:
     return out.value
 
 
+def Dist_graph_create_adjacent(sources, destinations, weighted=False):
+    """A distributed graph communicator over MPI_COMM_WORLD (MPI-3.1 7.5.4);
+    returns (err, comm)."""
+    src = (ctypes.c_int * max(len(sources), 1))(*sources)
+    dst = (ctypes.c_int * max(len(destinations), 1))(*destinations)
+    if weighted:
+        sw = (ctypes.c_int * max(len(sources), 1))(*([1] * len(sources)))
+        dw = (ctypes.c_int * max(len(destinations), 1))(*([1] * len(destinations)))
+    else:
+        sw = dw = ctypes.c_void_p(1)  # MPI_UNWEIGHTED
+    comm = ctypes.c_int(0)
+    err = _lib.minimpi().MPI_Dist_graph_create_adjacent(
+        COMM_WORLD, len(sources), src, sw, len(destinations), dst, dw, 0, 0,
+        ctypes.byref(comm))
+    return err, comm.value
+
+
+def Comm_free(comm: int) -> int:
+    c = ctypes.c_int(comm)
+    return _lib.minimpi().MPI_Comm_free(ctypes.byref(c))
+
+
+def _ints(v):
+    return (ctypes.c_int * max(len(v), 1))(*[int(x) for x in v])
+
+
+def _aints(v):
+    return (ctypes.c_ssize_t * max(len(v), 1))(*[int(x) for x in v])
+
+
+def Neighbor_alltoallv(sendbuf: int, sendcounts, sdispls, sendtype: int, recvbuf: int,
+                       recvcounts, rdispls, recvtype: int, comm: int) -> int:
+    """MPI_Neighbor_alltoallv: not interposed (the reference forwards it
+    unchanged), so this is the library's."""
+    return _lib.minimpi().MPI_Neighbor_alltoallv(
+        sendbuf, _ints(sendcounts), _ints(sdispls), sendtype, recvbuf, _ints(recvcounts),
+        _ints(rdispls), recvtype, comm)
+
+
+def Neighbor_alltoallw(sendbuf: int, sendcounts, sdispls, sendtypes, recvbuf: int,
+                       recvcounts, rdispls, recvtypes, comm: int,
+                       library: bool = False) -> int:
+    """MPI_Neighbor_alltoallw; displacements in bytes.  ``library=True``
+    calls the underlying MPI directly."""
+    lib = _lib.minimpi() if library else _lib.tempi()
+    return lib.MPI_Neighbor_alltoallw(
+        sendbuf, _ints(sendcounts), _aints(sdispls), _ints(sendtypes), recvbuf,
+        _ints(recvcounts), _aints(rdispls), _ints(recvtypes), comm)
+
+
 def describe(t: int):
     """TEMPI's canonical strided block for a type (tempi_describe)."""
     d = _lib.Desc()
