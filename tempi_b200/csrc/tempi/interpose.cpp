@@ -229,6 +229,9 @@ int MPI_Send(const void *buf, int count, MPI_Datatype datatype, int dest,
     return MPI_ERR_OTHER;
   if (env().disable)
     return libmpi.Send(buf, count, datatype, dest, tag, comm);
+  // earlier non-blocking sends reach the library first (non-overtaking)
+  if (int e = progress_sends())
+    return e;
   PtrInfo p = classify(buf);
   TypeRecord *r = p.device_accessible ? find_type(datatype) : nullptr;
   if (r && r->packable && r->desc.ndims >= 1 && count > 0) {
@@ -278,7 +281,10 @@ int MPI_Isend(const void *buf, int count, MPI_Datatype datatype, int dest,
     Method m = choose_method(*r, count);
     err = start_isend(*r, m, p.device_ptr, count, dest, tag, comm, request);
   } else {
-    err = libmpi.Isend(buf, count, datatype, dest, tag, comm, request);
+    // earlier managed sends reach the library first (non-overtaking)
+    err = progress_sends();
+    if (!err)
+      err = libmpi.Isend(buf, count, datatype, dest, tag, comm, request);
   }
   try_progress();
   return err;

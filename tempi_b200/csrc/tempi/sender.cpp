@@ -19,6 +19,7 @@
 
 #include "dispatch.hpp"
 
+#include <algorithm>
 #include <chrono>
 #include <map>
 #include <memory>
@@ -215,6 +216,7 @@ namespace {
 
 class AsyncOp {
 public:
+  uint64_t seq = 0; // creation order among managed operations
   virtual ~AsyncOp() {}
   virtual int wake() = 0;       // advance if possible
   virtual bool waiting() = 0;   // still needs wake() to reach its last state
@@ -395,6 +397,35 @@ public:
 std::mutex g_async_mu;
 std::map<MPI_Request, std::unique_ptr<AsyncOp>> g_active;
 uint32_t g_next = 0;
+uint64_t g_seq = 0;
+
+// Start the library sends of managed operations in creation order, each once
+// its pack has finished, stopping at the first whose pack has not: a send
+// never reaches the library ahead of an earlier one, which MPI's
+// non-overtaking rule needs (messages to one destination with one tag
+// arrive in the order sent).  Packs all run on one stream and so finish in
+// order, but a scan could otherwise see a later event complete that an
+// earlier query found pending.  Caller holds g_async_mu.  *pending: a send
+// is still waiting for its pack.
+int start_sends_in_order(bool *pending) {
+  std::vector<AsyncOp *> sends;
+  for (auto &kv : g_active)
+    if (kv.second->is_send() && kv.second->waiting())
+      sends.push_back(kv.second.get());
+  std::sort(sends.begin(), sends.end(),
+            [](const AsyncOp *a, const AsyncOp *b) { return a->seq < b->seq; });
+  *pending = false;
+  for (AsyncOp *op : sends) {
+    const int e = op->wake();
+    if (e)
+      return e;
+    if (op->waiting()) {
+      *pending = true;
+      break;
+    }
+  }
+  return MPI_SUCCESS;
+}
 
 MPI_Request make_request() {
   // minimpi keeps its own handles below 2^30; these sit above it
@@ -410,6 +441,7 @@ int start_isend(TypeRecord &r, Method m, const void *buf, int count, int dest,
     return op->err;
   std::lock_guard<std::mutex> l(g_async_mu);
   *request = make_request();
+  op->seq = g_seq++;
   g_active[*request] = std::move(op);
   counters().isend_managed++;
   return MPI_SUCCESS;
@@ -422,6 +454,7 @@ int start_irecv(TypeRecord &r, Method m, void *buf, int count, int source,
     return op->err;
   std::lock_guard<std::mutex> l(g_async_mu);
   *request = make_request();
+  op->seq = g_seq++;
   g_active[*request] = std::move(op);
   counters().irecv_managed++;
   return MPI_SUCCESS;
@@ -429,9 +462,10 @@ int start_irecv(TypeRecord &r, Method m, void *buf, int count, int source,
 
 int try_progress() {
   std::lock_guard<std::mutex> l(g_async_mu);
-  int first = MPI_SUCCESS;
+  bool pending = false;
+  int first = start_sends_in_order(&pending);
   for (auto &kv : g_active) {
-    if (kv.second->waiting()) {
+    if (!kv.second->is_send() && kv.second->waiting()) {
       int e = kv.second->wake();
       if (e && !first)
         first = e;
@@ -446,14 +480,9 @@ int progress_sends() {
     bool pending = false;
     {
       std::lock_guard<std::mutex> l(g_async_mu);
-      for (auto &kv : g_active) {
-        if (kv.second->is_send() && kv.second->waiting()) {
-          int e = kv.second->wake();
-          if (e)
-            return e;
-          pending |= kv.second->waiting();
-        }
-      }
+      int e = start_sends_in_order(&pending);
+      if (e)
+        return e;
     }
     if (!pending)
       return MPI_SUCCESS;
@@ -484,7 +513,13 @@ int wait_managed(MPI_Request *request, MPI_Status *status) {
   const double limit = env().wait_timeout_s;
   int err = MPI_SUCCESS;
   while (op->waiting()) {
-    err = op->wake();
+    if (op->is_send()) { // in order: the earlier sends go first
+      bool pending = false;
+      std::lock_guard<std::mutex> l(g_async_mu);
+      err = start_sends_in_order(&pending);
+    } else {
+      err = op->wake();
+    }
     if (err)
       break;
     if (!op->waiting())

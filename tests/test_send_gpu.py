@@ -171,3 +171,33 @@ def test_contiguous_device_send(cuda, mpi_init, mode):
         if var:
             os.environ.pop(var, None)
         _lib.tempi().tempi_reload_env()
+
+
+def test_non_overtaking_across_managed_and_library_sends(cuda, mpi_init):
+    """MPI's non-overtaking rule with one destination and one tag: a strided
+    Isend (packed by a kernel first, so its library send is deferred), then
+    a plain byte Isend, then another strided Isend.  Received in that order
+    -- and waited on out of order -- each message lands in its own
+    receive."""
+    import torch
+
+    vec = H.vector(200, 3, 7, H.named("BYTE")).commit()
+    a_np, c_np = H.splitmix_bytes(vec.o.extent, 1), H.splitmix_bytes(vec.o.extent, 3)
+    b_np = H.splitmix_bytes(57, 2)
+    a, b, c = dev(a_np), dev(b_np), dev(c_np)
+    ra = dev(np.full_like(a_np, 0xAA))
+    rb = dev(np.zeros_like(b_np))
+    rc = dev(np.full_like(c_np, 0xAA))
+    torch.cuda.synchronize()
+    e1, q1 = mpi.Isend(a.data_ptr(), 1, vec.h, tag=5)
+    e2, q2 = mpi.Isend(b.data_ptr(), 57, mpi.BYTE, tag=5)
+    e3, q3 = mpi.Isend(c.data_ptr(), 1, vec.h, tag=5)
+    e4, p1 = mpi.Irecv(ra.data_ptr(), 1, vec.h, tag=5)
+    e5, p2 = mpi.Irecv(rb.data_ptr(), 57, mpi.BYTE, tag=5)
+    e6, p3 = mpi.Irecv(rc.data_ptr(), 1, vec.h, tag=5)
+    assert (e1, e2, e3, e4, e5, e6) == (0,) * 6
+    for q in (q3, q1, q2, p3, p2, p1):  # out of order on purpose
+        assert mpi.Wait(q)[0] == 0
+    assert ra.cpu().numpy().tobytes() == expected(vec, a_np, 1).tobytes()
+    assert rb.cpu().numpy().tobytes() == b_np.tobytes()
+    assert rc.cpu().numpy().tobytes() == expected(vec, c_np, 1).tobytes()
