@@ -422,6 +422,55 @@ class BenchOp(ctypes.Structure):
 _driver = None
 
 
+def halo_exchange_bench(torch, stream, reps=20):
+    """Periodic halo exchange of a 256^3-double grid (radius 2) with
+    itself, the reference's bench_halo_exchange at world size 1: its
+    sequence (26 MPI_Pack, MPI_Neighbor_alltoallv of the packed bytes, 26
+    MPI_Unpack), one interposed MPI_Neighbor_alltoallw (the fused kernel),
+    and the fused kernel replayed from a CUDA graph.  All three must leave
+    the same grid."""
+    from tempi_b200 import halo
+
+    g = halo.Grid((256, 256, 256), 2)
+    sg = halo.SelfGraph(g)
+    n = len(sg.sendtypes)
+    base = torch.randint(0, 256, (g.nbytes,), dtype=torch.uint8, device="cuda")
+    grids = [base.clone() for _ in range(3)]
+    sendbuf = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
+    recvbuf = torch.zeros_like(sendbuf)
+    ints = lambda v: (ctypes.c_int * n)(*v)
+    st, rt, cnt, dsp = ints(sg.sendtypes), ints(sg.recvtypes), ints(sg.counts), ints(sg.displs)
+    out = (ctypes.c_float * reps)()
+    res = {"grid": "256^3 doubles, radius 2, periodic, one rank: 26 self-edges",
+           "bytes_exchanged": g.packed_bytes}
+    torch.cuda.synchronize()
+    for mode, key, gbuf in ((0, "pack_alltoallv_unpack_us", grids[0]),
+                            (1, "neighbor_alltoallw_us", grids[1])):
+        err = driver().tempi_bench_halo(mode, n, st, rt, cnt, dsp, gbuf.data_ptr(),
+                                        sendbuf.data_ptr(), recvbuf.data_ptr(),
+                                        g.packed_bytes, sg.comm, reps, out)
+        if err:
+            raise RuntimeError(f"halo exchange mode {mode} failed: {err}")
+        res[key] = round(1e3 * sorted(out)[reps // 2], 2)  # median
+    x = halo.HaloExchange([g], [grids[2].data_ptr()])
+    s = stream.cuda_stream
+    x.capture(s)
+    for _ in range(reps):
+        x.replay(s)
+    res["fused_graph_us"] = round(1e3 * time_events(torch, stream, lambda: x.replay(s), reps), 2)
+    x.close()
+    sg.close()
+    torch.cuda.synchronize()
+    # an exchange only writes ghost cells from interior cells, so repeating
+    # it changes nothing: however often each method ran, the grids agree
+    res["same_grid"] = bool(torch.equal(grids[0], grids[1]) and torch.equal(grids[0], grids[2]))
+    res["speedup_alltoallw_vs_reference_sequence"] = round(
+        res["pack_alltoallv_unpack_us"] / res["neighbor_alltoallw_us"], 2)
+    res["speedup_graph_vs_reference_sequence"] = round(
+        res["pack_alltoallv_unpack_us"] / res["fused_graph_us"], 2)
+    return res
+
+
 def driver():
     """The C benchmark driver (MPI call loops run from C)."""
     global _driver
@@ -434,6 +483,11 @@ def driver():
         _driver.tempi_bench_mpi_ops.argtypes = [
             ctypes.POINTER(BenchOp), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
             ctypes.c_size_t, ctypes.POINTER(ctypes.c_float)]
+        ip = ctypes.POINTER(ctypes.c_int)
+        _driver.tempi_bench_halo.argtypes = [
+            ctypes.c_int, ctypes.c_int, ip, ip, ip, ip, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+            ctypes.POINTER(ctypes.c_float)]
     return _driver
 
 
@@ -767,6 +821,8 @@ def run_ours(args):
     # the other ranks waiting at the final barrier
     solo = rank == 0 and world == 1
     halo_res = halo_bench(torch, side) if solo else None
+    if halo_res is not None:
+        halo_res["exchange"] = halo_exchange_bench(torch, side)
     # end to end: every rank at once, the whole job's rate from the slowest
     # rank's time (replicas: each rank moves its own copy of the workload)
     barrier()

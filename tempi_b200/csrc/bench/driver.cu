@@ -92,4 +92,58 @@ int tempi_bench_mpi_ops(const tempi_bench_op *ops, int n, int iters,
   return err;
 }
 
+// A periodic halo exchange of one grid with itself over a graph
+// communicator of n self-edges, `iters` times; ms_out[i] is step i's device
+// time (events on TEMPI's stream; every call below returns only when its
+// work is done).  mode 0: the reference's sequence (bin/bench_halo_exchange.cpp
+// :560-625): MPI_Pack of every send region into sendbuf, MPI_Neighbor_alltoallv
+// of the packed bytes, MPI_Unpack of every region from recvbuf.  mode 1: one
+// MPI_Neighbor_alltoallw with a send and a receive datatype per edge.
+int tempi_bench_halo(int mode, int n, const int *sendtypes,
+                     const int *recvtypes, const int *counts,
+                     const int *displs, void *grid, void *sendbuf,
+                     void *recvbuf, int packed_bytes, int comm, int iters,
+                     float *ms_out) {
+  cudaStream_t s = static_cast<cudaStream_t>(tempi_stream());
+  cudaEvent_t a, b;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess)
+    return 2;
+  int *ones = new int[n];
+  MPI_Aint *zeros = new MPI_Aint[n];
+  for (int i = 0; i < n; ++i) {
+    ones[i] = 1;
+    zeros[i] = 0;
+  }
+  int err = 0;
+  for (int it = 0; it < iters && !err; ++it) {
+    cudaEventRecord(a, s);
+    if (mode == 0) {
+      int pos = 0;
+      for (int i = 0; i < n && !err; ++i)
+        err = MPI_Pack(grid, 1, sendtypes[i], sendbuf, packed_bytes, &pos, comm);
+      if (!err)
+        err = MPI_Neighbor_alltoallv(sendbuf, counts, displs, MPI_BYTE,
+                                     recvbuf, counts, displs, MPI_BYTE, comm);
+      pos = 0;
+      for (int i = 0; i < n && !err; ++i)
+        err = MPI_Unpack(recvbuf, packed_bytes, &pos, grid, 1, recvtypes[i],
+                         comm);
+    } else {
+      err = MPI_Neighbor_alltoallw(grid, ones, zeros, sendtypes, grid, ones,
+                                   zeros, recvtypes, comm);
+    }
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms_out)
+      ms_out[it] = ms;
+  }
+  delete[] ones;
+  delete[] zeros;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return err;
+}
+
 } // extern "C"
