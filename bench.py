@@ -929,6 +929,27 @@ def run_profile_halo(args):
                       "unpack": bool(args.profile_unpack)}))
 
 
+def run_profile_exchange(args):
+    """A small case for ncu: the fused periodic halo exchange of the
+    256^3-double, radius-2 grid (26 copy pairs, one launch), launched
+    --profile-reps times."""
+    import torch
+
+    from tempi_b200 import halo, mpi
+
+    assert mpi.Init() == 0
+    g = halo.Grid((256, 256, 256), 2)
+    data = torch.randint(0, 256, (g.nbytes,), dtype=torch.uint8, device="cuda")
+    x = halo.HaloExchange([g], [data.data_ptr()])
+    torch.cuda.synchronize()
+    for _ in range(args.profile_reps):
+        x.launch()
+    torch.cuda.synchronize()
+    x.close()
+    print(json.dumps({"profile": "periodic halo exchange 256^3 doubles r=2", "pairs": 26,
+                      "bytes_copied": g.packed_bytes, "device_bytes": g.nbytes}))
+
+
 def run_host_link(args):
     """Host-link rates on this machine: the copy engines one way and both
     ways, the word kernel reading, writing and copying pinned host memory,
@@ -1022,9 +1043,13 @@ def main():
                     help="run only the batched halo kernel (for ncu)")
     ap.add_argument("--host-link", action="store_true",
                     help="measure the host-link rates and exit")
+    ap.add_argument("--profile-exchange", action="store_true",
+                    help="run only the fused halo-exchange kernel (for ncu)")
     args = ap.parse_args()
     if args.host_link:
         run_host_link(args)
+    elif args.profile_exchange:
+        run_profile_exchange(args)
     elif args.profile_halo:
         run_profile_halo(args)
     elif args.profile_point:

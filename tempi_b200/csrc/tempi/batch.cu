@@ -207,7 +207,7 @@ __device__ __forceinline__ void copy_pair_chunk(const CopyPair &r, uint32_t w0) 
       *reinterpret_cast<T *>(r.dst + dof[u]) = v[u];
 }
 
-__global__ void __launch_bounds__(kBatchThreads, 2)
+__global__ void __launch_bounds__(kBatchThreads, 3)
     k_batch_copy(const CopyPair *__restrict__ pairs, int npairs,
                  uint32_t total_chunks) {
   __shared__ CopyPair sp;
