@@ -114,6 +114,13 @@ def test_periodic_self_exchange_fused_alltoallw_and_plain(cuda, mpi_init, interi
     halo.exchange_alltoallw(sg, b.data_ptr())
     assert _lib.counter("neighbor_fused") == n0 + 1
     assert b.cpu().numpy().tobytes() == want.tobytes()
+    # the same call again (its region table is already on the device) on
+    # fresh data
+    data2 = H.splitmix_bytes(g.nbytes, radius + 41)
+    b.copy_(torch.from_numpy(data2))
+    torch.cuda.synchronize()
+    halo.exchange_alltoallw(sg, b.data_ptr())
+    assert b.cpu().numpy().tobytes() == oracle_exchange(g, data2).tobytes()
     # the reference's sequence through the interposer and the library
     c = torch.from_numpy(data_np).cuda()
     sendbuf = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
