@@ -21,13 +21,13 @@ Also reported on the same GPU in the same run:
              host memory over the link); `e2e.staged` is the alternative that
              copies every source span host->device, packs, copies the packed
              bytes back, and the reverse for the unpack
-  sendrecv   config 5: self-sends of strided device objects (4 KiB - 1 GiB)
+  sendrecv   self-sends of strided device objects (4 KiB - 1 GiB)
              by DEVICE, ONE_SHOT and STAGED, and what the learned model, the
              restated perf-table model and the fixed rules pick
   dispatch   a held-out sample (seed never trained on) of random layouts:
              total-time regret of the learned kernel-configuration choice
              and of the fixed rules against exhaustive measurement
-  config1    config 1 (vector 1024 x 64 B, stride 512) through the interposer
+  vector_1024x64  the 1024 x 64 B vector (stride 512) through the interposer
              on host buffers (the library's host pack) and on device buffers
   cpu_baseline  the oracle's C type-map walker (a port of what the underlying
              MPI's host MPI_Pack does) on one host core, on a bounded sample
@@ -591,7 +591,7 @@ def e2e_zero_copy(torch, sw, steps, warmup):
 
 
 def sendrecv_bench(torch, mpi, reps=2):
-    """Config 5: self-sends (MPI_Isend + MPI_Irecv + MPI_Wait x2) of strided
+    """Self-sends (MPI_Isend + MPI_Irecv + MPI_Wait x2) of strided
     device objects by each method, and the method each policy picks."""
     import time as _t
 
@@ -714,8 +714,8 @@ def dispatch_sample(torch, n=200, seed=777):
             "largest_losses": worst}
 
 
-def config1_bench(torch, mpi, reps=200):
-    """Config 1: MPI_Type_vector(1024, 64, 512, MPI_BYTE), incount 1, 512 KiB
+def vector_1024x64_bench(torch, mpi, reps=200):
+    """MPI_Type_vector(1024, 64, 512, MPI_BYTE), incount 1, 512 KiB
     of seeded random bytes.  With host buffers the interposed MPI_Pack hands
     the call to the underlying library (its host pack, as the reference does,
     src/pack.cpp:51-55); the same type on device buffers runs the kernel.
@@ -837,7 +837,7 @@ def run_ours(args):
         part["d2h_bytes_per_step"] *= world
     e2e = dict(e2e_zc, staged=e2e_staged)
     send_res = sendrecv_bench(torch, mpi) if solo and not args.no_sendrecv else None
-    c1_res = config1_bench(torch, mpi) if solo else None
+    c1_res = vector_1024x64_bench(torch, mpi) if solo else None
     disp_res = dispatch_sample(torch) if solo and not args.no_sendrecv else None
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
@@ -857,7 +857,7 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "e2e": e2e,
         "halo": halo_res,
-        "config1": c1_res,
+        "vector_1024x64": c1_res,
         "sendrecv": send_res,
         "dispatch": disp_res,
         "sweep": [{"p": r["label"], "k": r["kernel"], "pack_gbs": round(r["pack_gbs"], 1),

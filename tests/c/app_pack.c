@@ -1,7 +1,7 @@
 /* A plain MPI application, linked `-ltempi_b200 -lminimpi`: MPI_Pack and
    MPI_Type_commit resolve to the interposer, which reaches the library's
-   definitions through dlsym(RTLD_NEXT).  Packs config 1 (vector 1024 x 64 B,
-   stride 512 B) from host memory and checks every byte. */
+   definitions through dlsym(RTLD_NEXT).  Packs the 1024 x 64 B vector
+   (stride 512 B) from host memory and checks every byte. */
 #include <mpi.h>
 #include <stdio.h>
 #include <stdlib.h>

@@ -4,7 +4,7 @@ Each fixture is a seeded case of the pack path: a type (described without
 any MPI library), the seed and size of a random byte buffer, the object
 count, and the packed bytes that MPI type-map order gives.  The packed bytes
 come from the oracle's numpy type-map expansion (oracle/types.py), which
-follows the MPI-3.1 type constructors.  Shapes: config 1 of the benchmark
+follows the MPI-3.1 type constructors.  Shapes: the 1024 x 64 B vector of the benchmark
 (vector 1024 x 64 B, stride 512 B, truncated output is not stored -- only a
 hash), the reference's test/pack_unpack.cpp shapes, and a Fortran-order
 subarray.

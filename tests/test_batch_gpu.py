@@ -1,4 +1,4 @@
-"""Batched halo pack/unpack (benchmark config 3 at test sizes): one launch,
+"""Batched halo pack/unpack (the halo workload at test sizes): one launch,
 or one CUDA-graph replay, must write exactly what 26 per-region MPI_Pack
 calls write, and the unpack must fill exactly the ghost cells."""
 import numpy as np
@@ -97,7 +97,7 @@ def test_graph_replay_sees_new_data(cuda, mpi_init):
 
 def test_mixed_batch_of_8_grids(cuda, mpi_init):
     """Eight grids with log-uniform interiors and radius 1-3, 208 regions,
-    one launch (config 3's mixed batch at test sizes)."""
+    one launch (the mixed halo batch at test sizes)."""
     import torch
 
     rng = np.random.default_rng(3)

@@ -44,8 +44,8 @@ def test_no_mpi_library_is_linked_in():
     assert "minimpi" not in out and "libmpi" not in out
 
 
-def test_config1_host_pack_goes_to_library_and_is_exact(mpi_init):
-    """Config 1: vector(1024,64,512,BYTE) on host buffers, through the
+def test_vector_1024x64_host_pack_goes_to_library_and_is_exact(mpi_init):
+    """vector(1024,64,512,BYTE) on host buffers, through the
     interposed MPI_Pack, equals the oracle; unpack leaves 0xAA gaps alone."""
     t = H.make_2d_byte_vector(1024, 64, 512).commit()
     src = H.splitmix_bytes(512 * 1024, 0)

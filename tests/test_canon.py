@@ -27,7 +27,7 @@ def desc_pack(d, buf, incount, origin=0):
     return np.ascontiguousarray(v).ravel()
 
 
-def test_config1_descriptor(mpi_init):
+def test_vector_1024x64_descriptor(mpi_init):
     t = H.make_2d_byte_vector(1024, 64, 512).commit()
     err, d = mpi.describe(t.h)
     assert err == 0

@@ -46,7 +46,7 @@ def test_log2_known_answers():
     assert [I.log2_ceil(x) for x in (1, 2, 3, 4, 5, 1023, 1024, 1025)] == [0, 1, 2, 2, 3, 10, 10, 11]
 
 
-def test_config1_strided_block():
+def test_vector_1024x64_strided_block():
     # worked example: MPI_Type_vector(1024,64,512,MPI_BYTE)
     t = T.vector(1024, 64, 512, T.BYTE)
     assert (t.size, t.lb, t.extent) == (65536, 0, 523840)

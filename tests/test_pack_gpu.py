@@ -78,7 +78,7 @@ def test_reference_shapes(cuda, mpi_init, case):
     check_roundtrip(ty, count, pattern=True)
 
 
-def test_config1_device(cuda, mpi_init):
+def test_vector_1024x64_device(cuda, mpi_init):
     ty = H.make_2d_byte_vector(1024, 64, 512).commit()
     check_roundtrip(ty, 1, seed=0)
     assert _lib.counter("packs") > 0
@@ -369,7 +369,7 @@ SWEEP_3D = [(c, 256, 256) for c in (1, 2, 4, 8, 16, 64, 256)]
 @pytest.mark.parametrize("inner,rows", SWEEP_2D)
 @pytest.mark.parametrize("incount", [1, 16])
 def test_sweep_2d_full_size(cuda, mpi_init, inner, rows, incount):
-    """Benchmark config 2, 2-D: float subarrays of a 1024x1024 array at full
+    """The strided sweep, 2-D: float subarrays of a 1024x1024 array at full
     size, starts from a seed, compared with the oracle's C walker."""
     rng = np.random.default_rng(inner * 31 + incount)
     sc = int(rng.integers(0, 1024 - inner + 1))
@@ -388,7 +388,7 @@ def test_sweep_3d_full_size(cuda, mpi_init, inner, mid, outer):
 
 def test_sweep_equivalent_constructors(cuda, mpi_init):
     """The same pattern as a subarray, an hvector of vectors and a
-    contiguous of hvectors packs identically (config 2's variants)."""
+    contiguous of hvectors packs identically (the sweep's variants)."""
     C, r, c, sr, sc = 1024, 96, 24, 5, 13
     sub = H.subarray([1024, C], [r, c], [sr, sc], mpi.ORDER_C, H.named("FLOAT")).commit()
     hv = H.resized(H.hvector(r, 1, 4 * C, H.vector(1, c, c, H.named("FLOAT"))), 0, 4 * C * 1024).commit()

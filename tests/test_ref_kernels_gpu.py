@@ -53,7 +53,7 @@ def ref_launch(ref, sb, unpack, typed, packed, incount, stream=None):
 def cases():
     """(name, Ty, incount) where the reference's word size divides every
     stride, so its kernels are correct."""
-    out = [("config1_vector_1024x64_s512", H.make_2d_byte_vector(1024, 64, 512), 1)]
+    out = [("vector_1024x64_s512", H.make_2d_byte_vector(1024, 64, 512), 1)]
     out.append(("2d_float_sub_c64_r1024", H.subarray([1024, 1024], [1024, 64], [0, 128],
                                                      mpi.ORDER_C, H.named("FLOAT")), 4))
     out.append(("2d_float_sub_c256_r1024", H.subarray([1024, 1024], [1024, 256], [0, 512],

@@ -1,6 +1,6 @@
 """Self-sends of strided device objects through the interposed
 MPI_Send/MPI_Recv/MPI_Isend/MPI_Irecv/MPI_Wait, by each transfer method
-(benchmark config 5 at small sizes).  The reference only checks that these
+(the self-send workload at small sizes).  The reference only checks that these
 complete (test/isend.cu, test/send.cpp); here every received byte is
 compared with the oracle and gap bytes must keep their 0xAA fill."""
 import os
