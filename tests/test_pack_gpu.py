@@ -399,3 +399,108 @@ def test_sweep_equivalent_constructors(cuda, mpi_init):
     b, _, _ = pack_dev(hv, src, 1, origin=origin)
     c_, _, _ = pack_dev(ch, src, 1, origin=origin)
     assert a.tobytes() == b.tobytes() == c_.tobytes() == T.pack(sub.o, src, 1).tobytes()
+
+
+def _cudart():
+    import ctypes as C
+    import os as _os
+
+    import nvidia.cuda_runtime as cr
+
+    rt = C.CDLL(_os.path.join(list(cr.__path__)[0], "lib", "libcudart.so.12"))
+    rt.cudaMallocManaged.argtypes = [C.POINTER(C.c_void_p), C.c_size_t, C.c_uint]
+    rt.cudaFree.argtypes = [C.c_void_p]
+    rt.cudaDeviceSynchronize.argtypes = []
+    return rt
+
+
+@pytest.mark.parametrize("case", range(13))
+def test_reference_shapes_on_managed_memory(cuda, mpi_init, case):
+    """The reference's pack test allocates its buffers with cudaMallocManaged
+    (test/pack_unpack.cpp): the same shapes on managed memory go through the
+    interposer's GPU path, bit-exact both ways, gaps untouched."""
+    rt = _cudart()
+    ty, count = H.reference_pack_cases()[case]
+    ty.commit()
+    o = ty.o
+    lo, hi = H.span(o, count)
+    lo = min(lo, 0)
+    nbytes = hi - lo + 64
+    ptrs = []
+
+    def managed(n):
+        p = ctypes.c_void_p()
+        assert rt.cudaMallocManaged(ctypes.byref(p), max(n, 1), 1) == 0  # attach global
+        ptrs.append(p.value)
+        return p.value, np.ctypeslib.as_array((ctypes.c_uint8 * max(n, 1)).from_address(p.value))
+
+    try:
+        sp, src = managed(nbytes)
+        src[:] = (np.arange(nbytes) & 0xFF).astype(np.uint8)  # src[i] = (char)i
+        pp, packed = managed(o.size * count)
+        up, dst = managed(nbytes)
+        dst[:] = 0xAA
+        assert rt.cudaDeviceSynchronize() == 0
+        n0 = _lib.counter("packs")
+        err, pos = mpi.Pack(sp - lo, count, ty.h, pp, o.size * count)
+        assert err == 0 and pos == o.size * count, _lib.last_error()
+        assert _lib.counter("packs") == n0 + 1  # the GPU path, not the library
+        err, _ = mpi.Unpack(pp, o.size * count, up - lo, count, ty.h)
+        assert err == 0, _lib.last_error()
+        assert rt.cudaDeviceSynchronize() == 0
+        want = W.Walker(o).pack(src.copy(), count, origin=-lo)
+        assert packed[:pos].tobytes() == want.tobytes()
+        exp = np.full(nbytes, 0xAA, np.uint8)
+        W.Walker(o).unpack(want, exp, count, origin=-lo)
+        assert dst.tobytes() == exp.tobytes()
+    finally:
+        for p in ptrs:
+            rt.cudaFree(p)
+
+
+def test_offsets_beyond_4gib(cuda, mpi_init):
+    """Rows more than 4 GiB from the origin (the reference's >4 GiB case is
+    compiled out, test/pack_unpack.cpp:139-155): three 100-byte rows 2 GiB +
+    13 bytes apart, as one object and as two objects 3 GiB apart."""
+    import torch
+
+    step = (2 << 30) + 13
+    d = _lib.Desc.make(7, 3 * step, 100, [3], [step])
+    total = 7 + 2 * step + 100 + 256
+    buf = torch.zeros(total, dtype=torch.uint8, device="cuda")
+    rows = [H.splitmix_bytes(100, 60 + i) for i in range(3)]
+    for i, r in enumerate(rows):
+        buf[7 + i * step: 7 + i * step + 100] = torch.from_numpy(r).cuda()
+    out = torch.zeros(300, dtype=torch.uint8, device="cuda")
+    _lib.check(_lib.tempi().tempi_pack(ctypes.byref(d), buf.data_ptr(), 1, out.data_ptr(),
+                                        None, None))
+    torch.cuda.synchronize()
+    assert out.cpu().numpy().tobytes() == np.concatenate(rows).tobytes()
+    # unpack into the same places after clearing them; the bytes around stay 0
+    for i in range(3):
+        buf[7 + i * step: 7 + i * step + 100] = 0
+    _lib.check(_lib.tempi().tempi_unpack(ctypes.byref(d), out.data_ptr(), 1, buf.data_ptr(),
+                                          None, None))
+    torch.cuda.synchronize()
+    for i, r in enumerate(rows):
+        at = 7 + i * step
+        got = buf[at - 7: at + 107].cpu().numpy()
+        assert got[7:107].tobytes() == r.tobytes()
+        assert not got[:7].any() and not got[107:].any()
+    del buf
+    torch.cuda.empty_cache()
+    # two objects, the second at 3 GiB: rows at 3 GiB + 5 and 3 GiB + 5 + 1 GiB
+    d2 = _lib.Desc.make(5, 3 << 30, 64, [2], [1 << 30])
+    total = 5 + (3 << 30) + (1 << 30) + 64 + 64
+    buf = torch.zeros(total, dtype=torch.uint8, device="cuda")
+    offs = [5, 5 + (1 << 30), 5 + (3 << 30), 5 + (3 << 30) + (1 << 30)]
+    rows = [H.splitmix_bytes(64, 70 + i) for i in range(4)]
+    for o, r in zip(offs, rows):
+        buf[o: o + 64] = torch.from_numpy(r).cuda()
+    out = torch.zeros(256, dtype=torch.uint8, device="cuda")
+    _lib.check(_lib.tempi().tempi_pack(ctypes.byref(d2), buf.data_ptr(), 2, out.data_ptr(),
+                                        None, None))
+    torch.cuda.synchronize()
+    assert out.cpu().numpy().tobytes() == np.concatenate(rows).tobytes()
+    del buf
+    torch.cuda.empty_cache()
