@@ -5,6 +5,7 @@
 #include "tempi_b200.h"
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <atomic>
 #include <cstdint>
@@ -55,6 +56,16 @@ Counters &counters();
 
 // last kernel variant name, for tests and profiling
 void set_last_kernel(const char *name);
+
+// An NVTX range over a scope, as the reference marks its interposed calls
+// (src/pack.cpp:37,66): visible in Nsight Systems, free when no tool is
+// attached (NVTX3 is header-only and resolves its hooks lazily).
+struct TraceRange {
+  explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange &) = delete;
+  TraceRange &operator=(const TraceRange &) = delete;
+};
 
 // ---- launch geometry ------------------------------------------------------
 

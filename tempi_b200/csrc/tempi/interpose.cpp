@@ -111,6 +111,7 @@ int MPI_Finalize(void) {
 }
 
 int MPI_Type_commit(MPI_Datatype *datatype) {
+  TraceRange trace("MPI_Type_commit");
   if (!ready())
     return MPI_ERR_OTHER;
   int err = libmpi.Type_commit(datatype);
@@ -130,6 +131,7 @@ int MPI_Type_free(MPI_Datatype *datatype) {
 
 int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
              void *outbuf, int outsize, int *position, MPI_Comm comm) {
+  TraceRange trace("MPI_Pack");
   if (!ready())
     return MPI_ERR_OTHER;
   if (env().disable || env().no_pack)
@@ -177,6 +179,7 @@ int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
 
 int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
                int outcount, MPI_Datatype datatype, MPI_Comm comm) {
+  TraceRange trace("MPI_Unpack");
   if (!ready())
     return MPI_ERR_OTHER;
   if (env().disable || env().no_pack)
@@ -225,6 +228,7 @@ int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
 
 int MPI_Send(const void *buf, int count, MPI_Datatype datatype, int dest,
              int tag, MPI_Comm comm) {
+  TraceRange trace("MPI_Send");
   if (!ready())
     return MPI_ERR_OTHER;
   if (env().disable)
@@ -249,6 +253,7 @@ int MPI_Send(const void *buf, int count, MPI_Datatype datatype, int dest,
 
 int MPI_Recv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
              MPI_Comm comm, MPI_Status *status) {
+  TraceRange trace("MPI_Recv");
   if (!ready())
     return MPI_ERR_OTHER;
   if (env().disable)
@@ -270,6 +275,7 @@ int MPI_Recv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
 
 int MPI_Isend(const void *buf, int count, MPI_Datatype datatype, int dest,
               int tag, MPI_Comm comm, MPI_Request *request) {
+  TraceRange trace("MPI_Isend");
   if (!ready())
     return MPI_ERR_OTHER;
   if (env().disable)
@@ -292,6 +298,7 @@ int MPI_Isend(const void *buf, int count, MPI_Datatype datatype, int dest,
 
 int MPI_Irecv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
               MPI_Comm comm, MPI_Request *request) {
+  TraceRange trace("MPI_Irecv");
   if (!ready())
     return MPI_ERR_OTHER;
   if (env().disable)
@@ -324,6 +331,7 @@ int MPI_Neighbor_alltoallw(const void *sendbuf, const int sendcounts[],
                            const MPI_Datatype sendtypes[], void *recvbuf,
                            const int recvcounts[], const MPI_Aint rdispls[],
                            const MPI_Datatype recvtypes[], MPI_Comm comm) {
+  TraceRange trace("MPI_Neighbor_alltoallw");
   if (!ready())
     return MPI_ERR_OTHER;
   if (env().disable)
@@ -413,6 +421,7 @@ int MPI_Neighbor_alltoallw(const void *sendbuf, const int sendcounts[],
 }
 
 int MPI_Wait(MPI_Request *request, MPI_Status *status) {
+  TraceRange trace("MPI_Wait");
   if (!ready())
     return MPI_ERR_OTHER;
   if (env().disable || !request || !is_managed(*request)) {

@@ -3,6 +3,8 @@
 
 #include "runtime.hpp"
 
+#include <nvtx3/nvToolsExtCudaRt.h>
+
 #include <cstring>
 #include <string>
 
@@ -91,6 +93,8 @@ cudaStream_t pack_stream() {
         cudaSuccess) {
       cudaGetLastError();
       g_stream = nullptr;
+    } else {
+      nvtxNameCudaStreamA(g_stream, "TEMPI_pack");
     }
   }
   return g_stream;
@@ -103,6 +107,8 @@ cudaStream_t link_stream() {
     if (cudaStreamCreateWithFlags(&h, cudaStreamNonBlocking) != cudaSuccess) {
       cudaGetLastError();
       h = nullptr;
+    } else {
+      nvtxNameCudaStreamA(h, "TEMPI_link");
     }
   }
   return h;
