@@ -367,8 +367,20 @@ tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
   if (mode == Dispatch::LEARNED) {
     float f[TEMPI_MLP_IN], mean[TEMPI_MLP_OUT], spread[TEMPI_MLP_OUT];
     features(r.desc, incount, src_host, dst_host, f);
-    if (predict(f, mean, spread) == TEMPI_OK)
+    if (predict(f, mean, spread) == TEMPI_OK) {
       choice = pick(mean, spread, lo, lo + kNumConfigs, &trust, ok) - lo;
+      // one inference predicts both directions: keep the other's pick too,
+      // when the ensemble agrees on it
+      const int lo2 = unpack ? kPackOut : kUnpackOut;
+      bool trust2 = false;
+      const int other =
+          pick(mean, spread, lo2, lo2 + kNumConfigs, &trust2, ok) - lo2;
+      if (trust2) {
+        std::lock_guard<std::mutex> l(g_mu);
+        r.configs.emplace(config_key(incount, src_host, dst_host, !unpack),
+                          other);
+      }
+    }
   }
   if (mode == Dispatch::EXHAUSTIVE || (choice >= 0 && !trust)) {
     float t[kMeasured];
@@ -442,7 +454,8 @@ void on_commit(TypeRecord &r) {
   if (!r.packable || r.desc.size == 0 || env().dispatch != Dispatch::LEARNED ||
       !g_model.loaded || g_measuring)
     return;
-  // cached for device-to-device packs and unpacks
+  // cached for device-to-device packs and unpacks (one inference serves
+  // both unless the ensemble disagrees about the unpack)
   choose_config(r, 1, false, false, false);
   choose_config(r, 1, false, false, true);
 }
