@@ -76,8 +76,12 @@ typedef struct tempi_desc {
 /* Kernel choice for one launch.  Zero fields mean "let the library pick".
    kernel: 0 auto, 1 word kernel (a thread per vector word), 2 row kernel (a
    warp per row), 3 shift kernel (a group of `unroll` = 4/8/16/32 lanes per
-   row, 16-B accesses at any alignment).  width: vector bytes for kernels 1
-   and 2 (1,2,4,8,16; never above what the alignment proof allows). */
+   row, 16-B accesses at any alignment), 4 staged unpack (packed bytes
+   brought into shared memory by bulk asynchronous copies, 3 stages of 8 KB
+   per block, then scattered by vector words; unpack only, and only when the
+   packed base is 16-B aligned and the packed size a multiple of 16 -- other
+   calls take the automatic rules).  width: vector bytes for kernels 1, 2 and
+   4 (1,2,4,8,16; never above what the alignment proof allows). */
 typedef struct tempi_config {
   int32_t kernel;
   int32_t width;
@@ -260,11 +264,15 @@ int64_t tempi_kernel_launches(void);
 /* name of the kernel variant the last tempi_pack/unpack used */
 const char *tempi_last_kernel(void);
 /* value of a named counter (reference include/counters.hpp groups):
-   "packs", "unpacks", "lib_pack", "lib_unpack", "cached_types",
-   "send_device", "send_oneshot", "send_staged", "send_lib",
-   "recv_device", "recv_oneshot", "recv_staged", "recv_lib",
-   "isend_managed", "irecv_managed", "slab_hits", "slab_misses",
-   "dispatch_hit", "dispatch_miss"; -1 for an unknown name */
+   "kernel_launches", "packs", "unpacks", "pack_bytes", "unpack_bytes",
+   "lib_pack", "lib_unpack", "cached_types", "send_device", "send_oneshot",
+   "send_staged", "send_lib", "recv_device", "recv_oneshot", "recv_staged",
+   "recv_lib", "isend_managed", "irecv_managed", "dispatch_hit",
+   "dispatch_miss", "slab_hits", "slab_misses", "slab_bytes",
+   "host_link_copies", "send_contig_staged", "recv_contig_staged",
+   "neighbor_fused", "neighbor_isir", "neighbor_lib", and "staged_timeouts"
+   (bounded waits of the staged unpack kernel that gave up; read from the
+   device, so it synchronises); -1 for an unknown name */
 int64_t tempi_counter(const char *name);
 
 #ifdef __cplusplus

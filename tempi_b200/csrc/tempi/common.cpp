@@ -55,6 +55,8 @@ extern "C" const char *tempi_last_kernel(void) { return tempi::g_last_kernel; }
 extern "C" int64_t tempi_counter(const char *name) {
   if (!name)
     return -1;
+  if (std::string(name) == "staged_timeouts")
+    return tempi::staged_timeouts();
   auto &c = tempi::counters();
   const std::string n(name);
 #define C(x)                                                                   \

@@ -119,6 +119,9 @@ int launch_geometry(const Geometry &g, const char *strided_base, char *packed,
                     bool unpack, const tempi_config *cfg, cudaStream_t stream);
 
 int num_sms();
+// CTAs of the staged unpack (kernel 4) that gave up waiting on a bulk copy:
+// 0 unless something failed; -1 if it cannot be read
+int64_t staged_timeouts();
 
 // The copy batch's kernel (tempi_batch_create_copy) for one call, with its
 // pair table in a grow-only device buffer; launches on `s`, which the caller

@@ -266,6 +266,167 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Staged unpack (kernel 4): the contiguous packed side is pulled into shared
+// memory with bulk asynchronous copies (cp.async.bulk, completion counted on
+// an mbarrier), kStagedStages chunks in flight per CTA, and the threads
+// scatter each chunk's words to the typed rows from shared memory with
+// consecutive threads storing consecutive words.  Meant for rows whose
+// alignment forces narrow typed-side words: the plain kernels then keep too
+// few bytes of loads in flight.  The host launches it only when the packed
+// base is 16-B aligned and the packed size a multiple of 16 bytes, which is
+// what a bulk copy requires.  Every wait on an mbarrier is bounded (about a
+// second of SM clock); a CTA that gives up counts itself in
+// g_staged_timeouts, waits (bounded again) for its other copies and returns.
+constexpr int kStagedBytes = 8192;
+constexpr int kStagedStages = 3;
+constexpr int kStagedThreads = 256;
+
+__device__ int g_staged_timeouts;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void *dst, const void *src,
+                                          uint32_t bytes, uint64_t *bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                   smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::"
+               "bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_done(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile("{\n\t.reg .pred p;\n\t"
+               "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+               "selp.u32 %0, 1, 0, p;\n\t}"
+               : "=r"(ok)
+               : "r"(smem_u32(bar)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+
+// false after about 2^31 SM cycles (about a second) without completion
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar,
+                                                  uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_done(bar, parity)) {
+    if (clock64() - t0 > (1ll << 31))
+      return false;
+    __nanosleep(64);
+  }
+  return true;
+}
+
+template <int W, int ND>
+__global__ void __launch_bounds__(kStagedThreads)
+    k_unpack_staged(char *__restrict__ strided,
+                    const char *__restrict__ packed,
+                    const __grid_constant__ Geometry g, uint32_t nchunks,
+                    uint64_t total_bytes) {
+  using T = typename Word<W>::T;
+  __shared__ __align__(128) char stage[kStagedStages][kStagedBytes];
+  __shared__ __align__(8) uint64_t bar[kStagedStages];
+  __shared__ int gave_up;
+  auto chunk_bytes = [&](uint32_t c) {
+    const uint64_t left = total_bytes - uint64_t(c) * kStagedBytes;
+    return uint32_t(left < uint64_t(kStagedBytes) ? left : kStagedBytes);
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStagedStages; ++s)
+      mbar_init(&bar[s]);
+    gave_up = 0;
+    // the initialised barriers are visible to the copy engine's proxy
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int s = 0; s < kStagedStages; ++s) {
+      const uint32_t c = blockIdx.x + uint32_t(s) * gridDim.x;
+      if (c < nchunks)
+        bulk_load(stage[s], packed + uint64_t(c) * kStagedBytes,
+                  chunk_bytes(c), &bar[s]);
+    }
+  }
+  __syncthreads();
+  uint32_t it = 0;
+  for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x, ++it) {
+    const int s = int(it % kStagedStages);
+    const uint32_t parity = (it / kStagedStages) & 1;
+    if (!mbar_wait_bounded(&bar[s], parity))
+      gave_up = 1;
+    __syncthreads();
+    if (gave_up) {
+      if (threadIdx.x == 0) {
+        atomicAdd(&g_staged_timeouts, 1);
+        // the copies still counted on the other stages, bounded again
+        for (int k = 1; k < kStagedStages; ++k) {
+          const uint32_t ck = c + uint32_t(k) * gridDim.x;
+          if (ck < nchunks)
+            mbar_wait_bounded(&bar[(it + k) % kStagedStages],
+                              ((it + k) / kStagedStages) & 1);
+        }
+      }
+      return;
+    }
+    const uint32_t words = chunk_bytes(c) / W;
+    const uint32_t w0 = c * uint32_t(kStagedBytes / W);
+    const T *src = reinterpret_cast<const T *>(stage[s]);
+    for (uint32_t j = threadIdx.x; j < words; j += blockDim.x) {
+      const uint32_t w = w0 + j;
+      const uint32_t row = fastdiv(w, g.wdiv);
+      const uint32_t col = w - row * g.wpr;
+      *reinterpret_cast<T *>(strided + row_offset<ND>(row, g) +
+                             int64_t(col) * W) = src[j];
+    }
+    __syncthreads(); // every thread is done with stage s
+    if (threadIdx.x == 0) {
+      const uint32_t cn = c + uint32_t(kStagedStages) * gridDim.x;
+      if (cn < nchunks)
+        bulk_load(stage[s], packed + uint64_t(cn) * kStagedBytes,
+                  chunk_bytes(cn), &bar[s]);
+    }
+  }
+}
+
+using StagedFn = void (*)(char *, const char *, Geometry, uint32_t, uint64_t);
+
+int64_t staged_timeouts() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_staged_timeouts, sizeof(v)) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return v;
+}
+
+template <int W> StagedFn pick_staged_nd(uint32_t nd) {
+  switch (nd) {
+  case 0: return k_unpack_staged<W, 0>;
+  case 1: return k_unpack_staged<W, 1>;
+  case 2: return k_unpack_staged<W, 2>;
+  case 3: return k_unpack_staged<W, 3>;
+  case 4: return k_unpack_staged<W, 4>;
+  default: return k_unpack_staged<W, 5>;
+  }
+}
+
+StagedFn pick_staged(uint32_t width, uint32_t nd) {
+  switch (width) {
+  case 16: return pick_staged_nd<16>(nd);
+  case 8: return pick_staged_nd<8>(nd);
+  case 4: return pick_staged_nd<4>(nd);
+  case 2: return pick_staged_nd<2>(nd);
+  default: return pick_staged_nd<1>(nd);
+  }
+}
+
 using KernelFn = void (*)(char *, char *, Geometry);
 
 template <int L, bool UNPACK> KernelFn pick_shift(uint32_t nd) {
@@ -329,11 +490,11 @@ template <bool UNPACK> KernelFn pick(int kernel, uint32_t width, uint32_t nd) {
 }
 
 static const char *kernel_name(int kernel, uint32_t width, bool unpack) {
-  static char names[3][2][33][32];
+  static char names[4][2][33][32];
   static std::once_flag once;
   std::call_once(once, [] {
-    const char *k_names[3] = {"words", "rows", "shift"};
-    for (int k = 0; k < 3; ++k)
+    const char *k_names[4] = {"words", "rows", "shift", "staged"};
+    for (int k = 0; k < 4; ++k)
       for (int u = 0; u < 2; ++u)
         for (int w = 1; w <= 32; w *= 2)
           std::snprintf(names[k][u][w], 32, "%s_%s_%s%d", k_names[k],
@@ -451,6 +612,28 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
                     cudaStream_t stream) {
   const int sms = num_sms();
   int kernel = cfg ? cfg->kernel : 0;
+  if (kernel == 4) {
+    // the staged unpack, where its bulk copies are allowed: 16-B aligned
+    // packed base and a packed size that is a multiple of 16 bytes
+    const uint64_t bytes = uint64_t(g.rows) * uint64_t(g.block);
+    if (unpack && (reinterpret_cast<uintptr_t>(packed) & 15) == 0 &&
+        bytes % 16 == 0 && bytes > 0) {
+      const uint32_t nchunks =
+          uint32_t((bytes + kStagedBytes - 1) / kStagedBytes);
+      const uint32_t blocks =
+          std::max<uint32_t>(1, std::min<uint32_t>(nchunks, uint32_t(sms) * 8));
+      StagedFn fn = pick_staged(g.width, g.nd);
+      fn<<<blocks, kStagedThreads, 0, stream>>>(const_cast<char *>(strided),
+                                                packed, g, nchunks, bytes);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess)
+        return cuda_error(e, "staged unpack launch");
+      counters().kernel_launches++;
+      set_last_kernel(kernel_name(4, g.width, true));
+      return TEMPI_OK;
+    }
+    kernel = 0; // not eligible: the fixed rules below
+  }
   if (kernel < 1 || kernel > 3) {
     if (!unpack && g.width < 16 && g.block >= 128 && g.rows >= uint32_t(sms))
       kernel = 3; // misaligned wide rows: realign with funnel shifts

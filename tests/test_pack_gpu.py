@@ -504,3 +504,49 @@ def test_offsets_beyond_4gib(cuda, mpi_init):
     assert out.cpu().numpy().tobytes() == np.concatenate(rows).tobytes()
     del buf
     torch.cuda.empty_cache()
+
+
+def test_staged_unpack_matches_oracle(cuda, mpi_init):
+    """The staged unpack (kernel 4: packed chunks pulled into shared memory
+    by bulk copies, then scattered) at every typed-side width, with one to
+    three strided dimensions, several objects, sizes that leave a partial
+    last chunk, and a packed side that is not 16-B aligned (where it must
+    hand over to the plain kernels).  Gap bytes keep their 0xAA fill and no
+    bounded wait gives up."""
+    import torch
+
+    from tests.test_canon import desc_pack
+
+    cases = [  # (desc, incount): typed-side widths 4, 8, 1, 2, 16
+        (_lib.Desc.make(540, 1 << 20, 256, [1000], [1024]), 2),
+        (_lib.Desc.make(120, 300 * 1024, 64, [17, 300], [1024, 17 * 1024]), 1),
+        (_lib.Desc.make(3, 70000, 48, [1200], [57]), 1),
+        (_lib.Desc.make(2, 14000, 32, [5, 7, 9], [34, 200, 1500]), 3),
+        (_lib.Desc.make(0, 1 << 20, 4096, [60], [8192]), 2),
+    ]
+    before = _lib.counter("staged_timeouts")
+    for d, incount in cases:
+        span = d.start + d.extent * (incount - 1) + d.block + 64
+        for k in range(d.ndims):
+            span += d.strides[k] * (d.counts[k] - 1)
+        src_np = H.splitmix_bytes(span, d.block + incount)
+        want = desc_pack(d, src_np, incount)
+        assert want.size % 16 == 0
+        exp = np.full_like(src_np, 0xAA)
+        shape = [incount] + [d.counts[k] for k in reversed(range(d.ndims))] + [d.block]
+        strides = [d.extent] + [d.strides[k] for k in reversed(range(d.ndims))] + [1]
+        np.lib.stride_tricks.as_strided(exp[d.start:], shape=shape, strides=strides,
+                                        writeable=True)[...] = want.reshape(shape)
+        for mis in (0, 4):  # 4: the packed base is not 16-B aligned
+            packed = torch.zeros(want.size + 32, dtype=torch.uint8, device="cuda")
+            packed[mis: mis + want.size] = torch.from_numpy(want).cuda()
+            dst = torch.full((span,), 0xAA, dtype=torch.uint8, device="cuda")
+            cfg = _lib.Config(4, 0, 256, 0, 0, 0)
+            _lib.check(_lib.tempi().tempi_unpack(ctypes.byref(d), packed.data_ptr() + mis,
+                                                  incount, dst.data_ptr(), ctypes.byref(cfg),
+                                                  None))
+            sync()
+            kname = _lib.tempi().tempi_last_kernel().decode()
+            assert kname.startswith("staged") == (mis == 0), (kname, d.block)
+            assert host(dst).tobytes() == exp.tobytes(), (d.block, incount, mis)
+    assert _lib.counter("staged_timeouts") == before == 0
