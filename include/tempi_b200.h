@@ -176,22 +176,22 @@ int tempi_batch_run_static(const tempi_region *regions, int32_t n,
    Replaces the reference's measured-parameter tables (perf.json;
    src/internal/measure_system.cpp:106-299, include/measure_system.hpp:30-106)
    as the predictor behind the choice of kernel configuration and transfer
-   method.  An FP32 perceptron 12 -> 64 -> 64 -> 19 (ReLU), an ensemble of
+   method.  An FP32 perceptron 12 -> 64 -> 64 -> 23 (ReLU), an ensemble of
    `members` copies; one member's parameters are TEMPI_MLP_PARAMS floats laid
-   out W1[64][12] b1[64] W2[64][64] b2[64] W3[19][64] b3[19].  All pointers
+   out W1[64][12] b1[64] W2[64][64] b2[64] W3[23][64] b3[23].  All pointers
    below are device memory. */
 #define TEMPI_MLP_IN 12
 #define TEMPI_MLP_HIDDEN 64
-#define TEMPI_MLP_OUT 19
-#define TEMPI_MLP_PARAMS 6227
+#define TEMPI_MLP_OUT 23
+#define TEMPI_MLP_PARAMS 6487
 #define TEMPI_MLP_MEMBERS 5
 /* entries of tempi_measure's output: the model's outputs, then the fixed
    rules' pack and unpack */
-#define TEMPI_MEASURED 21
+#define TEMPI_MEASURED 25
 
 /* seeded uniform(+-1/sqrt(fan_in)) weights, zero biases */
 int tempi_mlp_init(float *params, int members, uint64_t seed);
-/* Adam on the masked mean squared error of y (n x 19; mask 1 = observed,
+/* Adam on the masked mean squared error of y (n x 23; mask 1 = observed,
    NULL = all observed) from x (n x 12); one CTA per member, mini-batches of
    `batch` <= 64 rows drawn with replacement.  loss_out (optional,
    members x epochs) receives each epoch's mean loss. */
@@ -199,7 +199,7 @@ int tempi_mlp_train(float *params, int members, const float *x,
                     const float *y, const float *mask, int n, int epochs,
                     int batch, float lr, uint64_t seed, float *loss_out,
                     void *stream);
-/* out[member][row][19] for n rows of x */
+/* out[member][row][23] for n rows of x */
 int tempi_mlp_predict(const float *params, int members, const float *x, int n,
                       float *out, void *stream);
 /* gradient (TEMPI_MLP_PARAMS floats) and loss of one member on rows
@@ -209,11 +209,12 @@ int tempi_mlp_grad(const float *params, const float *x, const float *y,
                    void *stream);
 
 /* ---- dispatch -------------------------------------------------------------
-   The model's nineteen outputs are log2 microseconds of: [0..7] a pack of the
-   objects with kernel configuration 0..7 (word kernel with 256, 512, 128
-   threads; row kernel; shift kernel with 4, 8, 16, 32 lanes per row),
-   [8..15] an unpack with configuration 0..7, [16..18] a self-send round trip
-   (MPI_Send + MPI_Recv) by DEVICE, ONE_SHOT, STAGED.  Pack and unpack are
+   The model's twenty-three outputs are log2 microseconds of: [0..9] a pack
+   of the objects with kernel configuration 0..9 (word kernel with 256, 512,
+   128 threads; row kernel; shift kernel with 4, 8, 16, 32 lanes per row;
+   staged kernel with 3 and with 8 CTAs per SM), [10..19] an unpack with
+   configuration 0..9, [20..22] a self-send round trip (MPI_Send + MPI_Recv)
+   by DEVICE, ONE_SHOT, STAGED.  Pack and unpack are
    chosen separately: they can prefer different kernels (a shift kernel packs
    misaligned rows from host memory well, but its partial end stores make it
    a poor unpacker into host memory).  `typed_host` / `packed_host`: the
@@ -225,7 +226,7 @@ int tempi_features(const tempi_desc *d, int64_t incount, int typed_host,
 /* time every candidate on scratch buffers shaped like the object (the
    exhaustive autotuner; reference bin/measure_system.cpp,
    src/internal/measure_system.cu:381-610).  what: bit 0 configurations,
-   bit 1 methods.  times_us[TEMPI_MEASURED]: the nineteen candidates above,
+   bit 1 methods.  times_us[TEMPI_MEASURED]: the twenty-three candidates above,
    then the fixed rules' (no model) pack and unpack; NaN where not
    measured. */
 int tempi_measure(const tempi_desc *d, int64_t incount, int typed_host,
@@ -235,8 +236,8 @@ int tempi_measure(const tempi_desc *d, int64_t incount, int typed_host,
 int tempi_dispatch_load(const char *model_path, const char *table_path);
 /* what a policy would choose.  mode 0: learned, 1: the reference's
    perf-table model restated (method only), 2: the fixed rules.
-   pack_config / unpack_config: 0..7 or -1 (fixed rules); method: 1 DEVICE,
-   2 ONE_SHOT, 3 STAGED.  predicted/spread (optional, 19 each): ensemble mean
+   pack_config / unpack_config: 0..9 or -1 (fixed rules); method: 1 DEVICE,
+   2 ONE_SHOT, 3 STAGED.  predicted/spread (optional, 23 each): ensemble mean
    and standard deviation, log2 microseconds (mode 0 only). */
 int tempi_dispatch_choose(const tempi_desc *d, int64_t incount,
                           int typed_host, int packed_host, int mode,

@@ -2,14 +2,14 @@
 
 Float64 restatement of the cost model's network and loss, to check the CUDA
 kernels' forward pass and gradients (tempi_mlp_predict, tempi_mlp_grad):
-12 -> 64 -> 64 -> 19 with ReLU, masked mean squared error.  Parameter layout
-per member: W1[64][12] b1[64] W2[64][64] b2[64] W3[19][64] b3[19].
+12 -> 64 -> 64 -> 23 with ReLU, masked mean squared error.  Parameter layout
+per member: W1[64][12] b1[64] W2[64][64] b2[64] W3[23][64] b3[23].
 """
 from __future__ import annotations
 
 import numpy as np
 
-IN, HID, OUT = 12, 64, 19
+IN, HID, OUT = 12, 64, 23
 SHAPES = [("W1", (HID, IN)), ("b1", (HID,)), ("W2", (HID, HID)), ("b2", (HID,)),
           ("W3", (OUT, HID)), ("b3", (OUT,))]
 P = sum(int(np.prod(s)) for _, s in SHAPES)

@@ -15,7 +15,7 @@
 
 namespace tempi {
 
-// the kernel configurations the model scores (outputs 0..7)
+// the kernel configurations the model scores (outputs 0..9)
 const tempi_config kCandidates[kNumConfigs] = {
     {1, 0, 256, 0, 0, 0},  // word kernel, 256 threads
     {1, 0, 512, 0, 0, 0},  // word kernel, 512 threads
@@ -25,6 +25,8 @@ const tempi_config kCandidates[kNumConfigs] = {
     {3, 0, 256, 8, 0, 0},  // shift kernel, 8 lanes per row
     {3, 0, 256, 16, 0, 0}, // shift kernel, 16 lanes per row
     {3, 0, 256, 32, 0, 0}, // shift kernel, 32 lanes per row
+    {4, 0, 256, 0, 3, 0},  // staged kernel, 3 CTAs per SM
+    {4, 0, 256, 0, 8, 0},  // staged kernel, 8 CTAs per SM
 };
 
 namespace {
@@ -299,6 +301,10 @@ bool eligible(const tempi_desc &d, int64_t incount, int k) {
     return g.block >= 64 && many_rows;
   if (c.kernel == 3)
     return g.block >= std::max<int64_t>(16, 4 * c.unroll) && many_rows;
+  if (c.kernel == 4) {
+    const int64_t bytes = int64_t(g.rows) * g.block;
+    return bytes >= (int64_t(64) << 10) && bytes % 16 == 0;
+  }
   return true;
 }
 

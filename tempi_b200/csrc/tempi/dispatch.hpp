@@ -16,7 +16,7 @@
 
 namespace tempi {
 
-constexpr int kNumConfigs = 8; // kernel configurations
+constexpr int kNumConfigs = 10; // kernel configurations
 constexpr int kNumMethods = 3; // DEVICE, ONE_SHOT, STAGED
 // model outputs: pack with configuration k, unpack with configuration k,
 // self-send by method m
@@ -32,7 +32,10 @@ static_assert(kFixedUnpack + 1 == kMeasured, "measured entries");
 
 // Whether candidate configuration k suits `incount` objects of `d`: a warp
 // per row needs rows of at least 64 B, a shift group of L lanes rows of at
-// least 4L bytes (16 B for L = 4), and both need at least two rows per SM.
+// least 4L bytes (16 B for L = 4), and both need at least two rows per SM;
+// the staged kernels need a packed size of at least 64 KiB that is a
+// multiple of 16 bytes (where a launch is not eligible for their bulk
+// copies it takes the fixed rules).
 // The harness measures only eligible candidates and the dispatcher chooses
 // only among them.
 bool eligible(const tempi_desc &d, int64_t incount, int k);
@@ -65,9 +68,9 @@ void on_commit(TypeRecord &r);
 // Load models from TEMPI_CACHE_DIR or next to the library (MPI_Init).
 void dispatch_init();
 
-// Time every candidate: times_us[0..7] = pack and [8..15] = unpack with each
-// kernel configuration, [16..18] = self-send round trip by each method,
-// [19] / [20] = pack / unpack by the fixed rules (NaN where not measured).
+// Time every candidate: times_us[0..9] = pack and [10..19] = unpack with
+// each kernel configuration, [20..22] = self-send round trip by each method,
+// [23] / [24] = pack / unpack by the fixed rules (NaN where not measured).
 // `what`: bit 0 configurations, bit 1 methods.
 int measure_candidates(const tempi_desc &d, int64_t incount, bool src_host,
                        bool dst_host, int what, int reps, float *times_us);

@@ -1,4 +1,4 @@
-// The learned cost model's network: a 12 -> 64 -> 64 -> 19 FP32 perceptron
+// The learned cost model's network: a 12 -> 64 -> 64 -> 23 FP32 perceptron
 // with ReLU hidden layers, trained and run by these kernels.  It replaces the
 // reference's measured-parameter tables (src/internal/measure_system.cpp,
 // interp_2d :223-299) as the predictor of pack and transfer times.

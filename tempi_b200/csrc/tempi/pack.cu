@@ -25,6 +25,7 @@
 //  * grids are a multiple of the SM count and grid-stride over the work.
 
 #include "internal.hpp"
+#include "runtime.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -395,7 +396,115 @@ __global__ void __launch_bounds__(kStagedThreads)
   }
 }
 
+// The staged pack: the mirror of k_unpack_staged for geometries whose every
+// row, stride and base is 16-B aligned (width 16).  Chunk c of the packed
+// stream is gathered into shared memory by one bulk copy per row piece it
+// covers -- the lanes of warp 0 issue the pieces in parallel, all counted on
+// the chunk's mbarrier -- and the threads then write the chunk to the packed
+// buffer with coalesced 16-B stores.  Same bounded waits and give-up path as
+// the staged unpack.
+template <int ND>
+__global__ void __launch_bounds__(kStagedThreads)
+    k_pack_staged(const char *__restrict__ strided, char *__restrict__ packed,
+                  const __grid_constant__ Geometry g, uint32_t nchunks,
+                  uint64_t total_bytes) {
+  __shared__ __align__(128) char stage[kStagedStages][kStagedBytes];
+  __shared__ __align__(8) uint64_t bar[kStagedStages];
+  __shared__ int gave_up;
+  const uint64_t block = uint64_t(g.block);
+  auto chunk_bytes = [&](uint32_t c) {
+    const uint64_t left = total_bytes - uint64_t(c) * kStagedBytes;
+    return uint32_t(left < uint64_t(kStagedBytes) ? left : kStagedBytes);
+  };
+  // warp 0 only: the row pieces of chunk c into stage s
+  auto gather = [&](uint32_t c, int s) {
+    const uint32_t lane = threadIdx.x;
+    const uint64_t p0 = uint64_t(c) * kStagedBytes;
+    const uint32_t n = chunk_bytes(c);
+    if (lane == 0)
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::
+                       "r"(smem_u32(&bar[s])),
+                   "r"(n)
+                   : "memory");
+    __syncwarp();
+    const uint32_t row0 = uint32_t(p0 / block);
+    const uint64_t off0 = p0 - uint64_t(row0) * block;
+    const uint64_t first = block - off0; // bytes of the first row's piece
+    for (uint32_t k = lane;; k += 32) {
+      // piece k: row row0 + k, at chunk offset d, in-row offset o
+      const uint64_t d = k == 0 ? 0 : first + uint64_t(k - 1) * block;
+      if (d >= n)
+        break;
+      const uint64_t o = k == 0 ? off0 : 0;
+      const uint64_t len = block - o < n - d ? block - o : n - d;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+          " [%0], [%1], %2, [%3];" ::"r"(smem_u32(stage[s] + d)),
+          "l"(strided + row_offset<ND>(row0 + k, g) + o), "r"(uint32_t(len)),
+          "r"(smem_u32(&bar[s]))
+          : "memory");
+    }
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStagedStages; ++s)
+      mbar_init(&bar[s]);
+    gave_up = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x < 32)
+    for (int s = 0; s < kStagedStages; ++s) {
+      const uint32_t c = blockIdx.x + uint32_t(s) * gridDim.x;
+      if (c < nchunks)
+        gather(c, s);
+    }
+  uint32_t it = 0;
+  for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x, ++it) {
+    const int s = int(it % kStagedStages);
+    const uint32_t parity = (it / kStagedStages) & 1;
+    if (!mbar_wait_bounded(&bar[s], parity))
+      gave_up = 1;
+    __syncthreads();
+    if (gave_up) {
+      if (threadIdx.x == 0) {
+        atomicAdd(&g_staged_timeouts, 1);
+        for (int k = 1; k < kStagedStages; ++k) {
+          const uint32_t ck = c + uint32_t(k) * gridDim.x;
+          if (ck < nchunks)
+            mbar_wait_bounded(&bar[(it + k) % kStagedStages],
+                              ((it + k) / kStagedStages) & 1);
+        }
+      }
+      return;
+    }
+    const uint32_t words = chunk_bytes(c) / 16;
+    const uint4 *src = reinterpret_cast<const uint4 *>(stage[s]);
+    uint4 *dst = reinterpret_cast<uint4 *>(packed + uint64_t(c) * kStagedBytes);
+    for (uint32_t j = threadIdx.x; j < words; j += blockDim.x)
+      dst[j] = src[j];
+    __syncthreads(); // every thread is done with stage s
+    if (threadIdx.x < 32) {
+      const uint32_t cn = c + uint32_t(kStagedStages) * gridDim.x;
+      if (cn < nchunks)
+        gather(cn, s);
+    }
+  }
+}
+
 using StagedFn = void (*)(char *, const char *, Geometry, uint32_t, uint64_t);
+using StagedPackFn = void (*)(const char *, char *, Geometry, uint32_t,
+                              uint64_t);
+
+StagedPackFn pick_staged_pack(uint32_t nd) {
+  switch (nd) {
+  case 0: return k_pack_staged<0>;
+  case 1: return k_pack_staged<1>;
+  case 2: return k_pack_staged<2>;
+  case 3: return k_pack_staged<3>;
+  case 4: return k_pack_staged<4>;
+  default: return k_pack_staged<5>;
+  }
+}
 
 int64_t staged_timeouts() {
   int v = 0;
@@ -612,27 +721,41 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
                     cudaStream_t stream) {
   const int sms = num_sms();
   int kernel = cfg ? cfg->kernel : 0;
-  if (kernel == 4) {
-    // the staged unpack, where its bulk copies are allowed: 16-B aligned
-    // packed base and a packed size that is a multiple of 16 bytes
-    const uint64_t bytes = uint64_t(g.rows) * uint64_t(g.block);
-    if (unpack && (reinterpret_cast<uintptr_t>(packed) & 15) == 0 &&
-        bytes % 16 == 0 && bytes > 0) {
-      const uint32_t nchunks =
-          uint32_t((bytes + kStagedBytes - 1) / kStagedBytes);
-      const uint32_t blocks =
-          std::max<uint32_t>(1, std::min<uint32_t>(nchunks, uint32_t(sms) * 8));
-      StagedFn fn = pick_staged(g.width, g.nd);
-      fn<<<blocks, kStagedThreads, 0, stream>>>(const_cast<char *>(strided),
-                                                packed, g, nchunks, bytes);
-      cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess)
-        return cuda_error(e, "staged unpack launch");
-      counters().kernel_launches++;
-      set_last_kernel(kernel_name(4, g.width, true));
-      return TEMPI_OK;
-    }
-    kernel = 0; // not eligible: the fixed rules below
+  // the staged kernels (4), where their bulk copies are allowed: unpack
+  // needs a 16-B aligned packed base and a packed size that is a multiple of
+  // 16 bytes; pack needs every row piece 16-B aligned on both sides (width
+  // 16).  Both sides must be device memory proper: host-mapped and managed
+  // buffers take the plain kernels.
+  const uint64_t bytes = uint64_t(g.rows) * uint64_t(g.block);
+  const bool wide = g.width == 16 && bytes >= (uint64_t(32) << 20);
+  const bool narrow_unpack =
+      unpack && bytes >= (uint64_t(1) << 20) && g.block <= 512;
+  if ((kernel == 4 || ((kernel < 1 || kernel > 4) && (wide || narrow_unpack))) &&
+      bytes % 16 == 0 &&
+      (unpack ? (reinterpret_cast<uintptr_t>(packed) & 15) == 0
+              : g.width == 16) &&
+      classify(strided).is_device && classify(packed).is_device) {
+    const uint32_t nchunks =
+        uint32_t((bytes + kStagedBytes - 1) / kStagedBytes);
+    // measured on the strided sweep: 3 CTAs per SM for long aligned
+    // streams, a full SM (8 CTAs of 256 threads) for narrow scatters
+    const int bps = (cfg && cfg->blocks_per_sm >= 1 && cfg->blocks_per_sm <= 8)
+                        ? cfg->blocks_per_sm
+                        : wide ? 3 : 8;
+    const uint32_t blocks = std::max<uint32_t>(
+        1, std::min<uint32_t>(nchunks, uint32_t(sms) * uint32_t(bps)));
+    if (unpack)
+      pick_staged(g.width, g.nd)<<<blocks, kStagedThreads, 0, stream>>>(
+          const_cast<char *>(strided), packed, g, nchunks, bytes);
+    else
+      pick_staged_pack(g.nd)<<<blocks, kStagedThreads, 0, stream>>>(
+          strided, packed, g, nchunks, bytes);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+      return cuda_error(e, "staged kernel launch");
+    counters().kernel_launches++;
+    set_last_kernel(kernel_name(4, g.width, unpack));
+    return TEMPI_OK;
   }
   if (kernel < 1 || kernel > 3) {
     if (!unpack && g.width < 16 && g.block >= 128 && g.rows >= uint32_t(sms))

@@ -10,9 +10,9 @@ equivalent:
    {1,2,4,8,16}, totals 1 KiB - 256 MiB log-uniform, typed and packed
    buffers in device or mapped pinned host memory) and times every
    candidate on each with tempi_measure: a pack and an unpack with each of
-   eight kernel configurations and with the fixed rules, and -- on a
+   ten kernel configurations and with the fixed rules, and -- on a
    subset -- the three transfer methods;
-2. trains the cost model (a 5-member FP32 MLP ensemble, 12 -> 64 -> 64 -> 19)
+2. trains the cost model (a 5-member FP32 MLP ensemble, 12 -> 64 -> 64 -> 23)
    on the GPU with tempi_mlp_train;
 3. measures the reference's table model on this machine (pack/unpack
    tables over 2^(2i+6) bytes x 2^j-byte blocks at a 512-byte stride,
@@ -43,11 +43,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 MODELS = os.path.join(HERE, "models")
 MODEL_FILE = "tempi_b200_dispatch.bin"
 TABLE_FILE = "tempi_b200_table.bin"
-N_CFG, N_METH = 8, 3
+N_CFG, N_METH = 10, 3
 PACK, UNPACK, METH = 0, N_CFG, 2 * N_CFG      # model output offsets
-N_OUT = 2 * N_CFG + N_METH                    # 19
+N_OUT = 2 * N_CFG + N_METH                    # 23
 FIXED_PACK, FIXED_UNPACK = N_OUT, N_OUT + 1   # measured after the outputs
-N_MEAS = N_OUT + 2                            # 21
+N_MEAS = N_OUT + 2                            # 25
 P = (12 * 64 + 64) + (64 * 64 + 64) + (64 * N_OUT + N_OUT)
 
 

@@ -27,9 +27,9 @@ def model(cuda, mpi_init):
 
 
 def test_measure_covers_eligible_candidates(model):
-    """Packs ([0..7]) and unpacks ([8..15]) are timed apart for every
-    eligible configuration, transfers by the three methods ([16..18]), and
-    the fixed rules' pack and unpack ([19], [20])."""
+    """Packs ([0..9]) and unpacks ([10..19]) are timed apart for every
+    eligible configuration, transfers by the three methods ([20..22]), and
+    the fixed rules' pack and unpack ([23], [24])."""
     lib = _lib.tempi()
     t = (ctypes.c_float * DT.N_MEAS)()
     d = _lib.Desc.make(4, 1 << 22, 1000, [2000], [2048])
@@ -39,8 +39,9 @@ def test_measure_covers_eligible_candidates(model):
     d = _lib.Desc.make(0, 1 << 20, 1 << 20, [], [])  # one contiguous block
     _lib.check(lib.tempi_measure(ctypes.byref(d), 1, 0, 0, 1, 2, t))
     v = np.frombuffer(t, np.float32)
-    for lo in (DT.PACK, DT.UNPACK):  # only the word kernels suit one block
+    for lo in (DT.PACK, DT.UNPACK):  # the word and staged kernels suit one block
         assert np.isfinite(v[lo:lo + 3]).all() and np.isnan(v[lo + 3:lo + 8]).all()
+        assert np.isfinite(v[lo + 8:lo + 10]).all()
     assert np.isnan(v[DT.METH:DT.METH + 3]).all()
     assert np.isfinite(v[DT.FIXED_PACK]) and np.isfinite(v[DT.FIXED_UNPACK])
 
@@ -58,7 +59,7 @@ def test_choice_is_eligible_and_pack_stays_exact(model):
         _lib.check(_lib.tempi().tempi_dispatch_choose(ctypes.byref(d), 2, 0, 0, 0,
                                                        ctypes.byref(pc), ctypes.byref(uc),
                                                        ctypes.byref(mi), pred, None))
-        assert 0 <= pc.value < 8 and 0 <= uc.value < 8 and 1 <= mi.value <= 3
+        assert 0 <= pc.value < DT.N_CFG and 0 <= uc.value < DT.N_CFG and 1 <= mi.value <= 3
         assert np.isfinite(np.frombuffer(pred, np.float32)).all()
         import torch
 
@@ -90,7 +91,7 @@ def test_learned_beats_fixed_rules_on_fresh_layouts(model):
                                               ctypes.byref(pc), ctypes.byref(uc),
                                               ctypes.byref(mi), None, None))
         v = np.frombuffer(t, np.float32)
-        tp, tu = v[DT.PACK:DT.PACK + 8], v[DT.UNPACK:DT.UNPACK + 8]
+        tp, tu = v[DT.PACK:DT.PACK + DT.N_CFG], v[DT.UNPACK:DT.UNPACK + DT.N_CFG]
         B.append(np.nanmin(tp) + np.nanmin(tu))
         L.append(tp[pc.value] + tu[uc.value])
         F.append(v[DT.FIXED_PACK] + v[DT.FIXED_UNPACK])

@@ -550,3 +550,45 @@ def test_staged_unpack_matches_oracle(cuda, mpi_init):
             assert kname.startswith("staged") == (mis == 0), (kname, d.block)
             assert host(dst).tobytes() == exp.tobytes(), (d.block, incount, mis)
     assert _lib.counter("staged_timeouts") == before == 0
+
+
+def test_staged_pack_matches_oracle(cuda, mpi_init):
+    """The staged pack (kernel 4 on the pack side: row pieces gathered into
+    shared memory by bulk copies, written out with coalesced stores) on
+    16-B aligned geometries: rows of 16 B (hundreds of pieces per chunk),
+    rows that chunks cut in the middle, a contiguous run with a partial last
+    chunk, and enough chunks that each CTA cycles its stages several times
+    (one CTA per SM).  A geometry narrower than 16 B hands over to the plain
+    kernels.  Bytes past the packed size stay untouched and no bounded wait
+    gives up."""
+    import torch
+
+    from tests.test_canon import desc_pack
+
+    cases = [  # (desc, incount, staged)
+        (_lib.Desc.make(0, 1 << 20, 4096, [60], [8192]), 2, True),
+        (_lib.Desc.make(32, 64 * 1040 + 64, 400, [64], [1040]), 3, True),
+        (_lib.Desc.make(16, 1 << 20, 16, [7, 9, 5], [48, 1024, 16384]), 4, True),
+        (_lib.Desc.make(0, (8 << 20) + 48, (8 << 20) + 48, [], []), 1, True),
+        (_lib.Desc.make(4, 1 << 20, 4096, [60], [8192]), 1, False),
+    ]
+    before = _lib.counter("staged_timeouts")
+    for d, incount, staged in cases:
+        span = d.start + d.extent * (incount - 1) + d.block + 64
+        for k in range(d.ndims):
+            span += d.strides[k] * (d.counts[k] - 1)
+        src_np = H.splitmix_bytes(span, d.block + incount + 5)
+        want = desc_pack(d, src_np, incount)
+        src = torch.from_numpy(src_np).cuda()
+        for bps in (1, 8):
+            packed = torch.full((want.size + 256,), 0x5A, dtype=torch.uint8, device="cuda")
+            cfg = _lib.Config(4, 0, 256, 0, bps, 0)
+            _lib.check(_lib.tempi().tempi_pack(ctypes.byref(d), src.data_ptr(), incount,
+                                                packed.data_ptr(), ctypes.byref(cfg), None))
+            sync()
+            kname = _lib.tempi().tempi_last_kernel().decode()
+            assert kname.startswith("staged") == staged, (kname, d.block)
+            got = host(packed)
+            assert got[:want.size].tobytes() == want.tobytes(), (d.block, incount, bps)
+            assert (got[want.size:] == 0x5A).all(), (d.block, incount, bps)
+    assert _lib.counter("staged_timeouts") == before == 0
