@@ -272,9 +272,17 @@ const char *tempi_last_kernel(void);
    "dispatch_miss", "slab_hits", "slab_misses", "slab_bytes",
    "host_link_copies", "send_contig_staged", "recv_contig_staged",
    "neighbor_fused", "neighbor_isir", "neighbor_lib", and "staged_timeouts"
-   (bounded waits of the staged unpack kernel that gave up; read from the
-   device, so it synchronises); -1 for an unknown name */
+   (staged launches whose bounded waits gave up, as far as the host has seen:
+   see tempi_staged_check); -1 for an unknown name */
 int64_t tempi_counter(const char *name);
+/* The staged kernels (kernel 4) wait on their bulk copies with a bound of
+   about a second; a kernel that gives up leaves its chunks uncopied and sets
+   a failure word in pinned host memory.  After synchronising the stream of a
+   tempi_pack / tempi_unpack call, this returns TEMPI_ERR_TIMEOUT if any staged
+   kernel gave up since the last check (and clears the word), else TEMPI_OK.
+   The interposed MPI calls check it themselves and return MPI_ERR_OTHER.  No
+   reference counterpart: the reference's kernels have no waits. */
+int tempi_staged_check(void);
 
 #ifdef __cplusplus
 }

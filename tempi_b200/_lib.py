@@ -187,6 +187,7 @@ _TEMPI_SIGS = {
     "tempi_kernel_launches": (c_int64, []),
     "tempi_last_kernel": (ctypes.c_char_p, []),
     "tempi_counter": (c_int64, [ctypes.c_char_p]),
+    "tempi_staged_check": (c_int, []),
     "tempi_stream": (c_void_p, []),
     "tempi_features": (c_int, [P(Desc), c_int64, c_int, c_int, c_void_p]),
     "tempi_measure": (c_int, [P(Desc), c_int64, c_int, c_int, c_int, c_int, c_void_p]),

@@ -119,9 +119,13 @@ int launch_geometry(const Geometry &g, const char *strided_base, char *packed,
                     bool unpack, const tempi_config *cfg, cudaStream_t stream);
 
 int num_sms();
-// CTAs of the staged unpack (kernel 4) that gave up waiting on a bulk copy:
-// 0 unless something failed; -1 if it cannot be read
+// Staged launches (kernel 4) that gave up waiting on a bulk copy, counted
+// once the host has seen their failure word (0 unless something failed).
 int64_t staged_timeouts();
+// After synchronising the stream of a staged launch: whether a staged kernel
+// gave up since the last call (its output is then incomplete).  Clears the
+// failure word.
+bool staged_failed();
 
 // The copy batch's kernel (tempi_batch_create_copy) for one call, with its
 // pair table in a grow-only device buffer; launches on `s`, which the caller

@@ -170,6 +170,8 @@ int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
     cudaError_t ce = cudaStreamSynchronize(s);
     if (ce != cudaSuccess)
       e = cuda_error(ce, "MPI_Pack synchronize");
+    else
+      e = tempi_staged_check();
   }
   if (e)
     return to_mpi(e);
@@ -219,6 +221,8 @@ int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
     cudaError_t ce = cudaStreamSynchronize(s);
     if (ce != cudaSuccess)
       e = cuda_error(ce, "MPI_Unpack synchronize");
+    else
+      e = tempi_staged_check();
   }
   if (e)
     return to_mpi(e);

@@ -167,6 +167,9 @@ int measure_candidates(const tempi_desc &d, int64_t incount, bool src_host,
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
       return cuda_error(e, "measure configurations");
+    if (staged_failed())
+      return set_error(TEMPI_ERR_TIMEOUT,
+                       "measure: a staged kernel gave up on its bulk copies");
   }
   if ((what & 2) && !src_host && incount <= INT32_MAX) {
     void *typed2 = get(g_typed2, size_t(span), false);

@@ -28,6 +28,7 @@
 #include "runtime.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -276,13 +277,24 @@ __global__ void __launch_bounds__(256)
 // few bytes of loads in flight.  The host launches it only when the packed
 // base is 16-B aligned and the packed size a multiple of 16 bytes, which is
 // what a bulk copy requires.  Every wait on an mbarrier is bounded (about a
-// second of SM clock); a CTA that gives up counts itself in
-// g_staged_timeouts, waits (bounded again) for its other copies and returns.
+// second of SM clock); a CTA that gives up sets the failure word of
+// StagedCtl (mapped pinned host memory, read by the host after it
+// synchronises: staged_failed), waits (bounded again) for its other copies
+// and returns, leaving its chunks uncopied.
 constexpr int kStagedBytes = 8192;
 constexpr int kStagedStages = 3;
 constexpr int kStagedThreads = 256;
 
-__device__ int g_staged_timeouts;
+struct StagedCtl {
+  int *fail;          // device address of the host-mapped failure word
+  uint32_t shortfall; // bytes each chunk's barrier expects beyond its copies:
+                      // 0, except to exercise the give-up path in tests
+};
+
+__device__ __forceinline__ void staged_give_up(const StagedCtl &ctl) {
+  *reinterpret_cast<volatile int *>(ctl.fail) = 1;
+  __threadfence_system();
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -293,11 +305,14 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar) {
                : "memory");
 }
 
+// one bulk copy of `bytes` into shared memory, its barrier told to expect
+// `bytes + shortfall`
 __device__ __forceinline__ void bulk_load(void *dst, const void *src,
-                                          uint32_t bytes, uint64_t *bar) {
+                                          uint32_t bytes, uint32_t shortfall,
+                                          uint64_t *bar) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
                    smem_u32(bar)),
-               "r"(bytes)
+               "r"(bytes + shortfall)
                : "memory");
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::"
                "bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
@@ -333,7 +348,7 @@ __global__ void __launch_bounds__(kStagedThreads)
     k_unpack_staged(char *__restrict__ strided,
                     const char *__restrict__ packed,
                     const __grid_constant__ Geometry g, uint32_t nchunks,
-                    uint64_t total_bytes) {
+                    uint64_t total_bytes, StagedCtl ctl) {
   using T = typename Word<W>::T;
   __shared__ __align__(128) char stage[kStagedStages][kStagedBytes];
   __shared__ __align__(8) uint64_t bar[kStagedStages];
@@ -352,7 +367,7 @@ __global__ void __launch_bounds__(kStagedThreads)
       const uint32_t c = blockIdx.x + uint32_t(s) * gridDim.x;
       if (c < nchunks)
         bulk_load(stage[s], packed + uint64_t(c) * kStagedBytes,
-                  chunk_bytes(c), &bar[s]);
+                  chunk_bytes(c), ctl.shortfall, &bar[s]);
     }
   }
   __syncthreads();
@@ -365,7 +380,7 @@ __global__ void __launch_bounds__(kStagedThreads)
     __syncthreads();
     if (gave_up) {
       if (threadIdx.x == 0) {
-        atomicAdd(&g_staged_timeouts, 1);
+        staged_give_up(ctl);
         // the copies still counted on the other stages, bounded again
         for (int k = 1; k < kStagedStages; ++k) {
           const uint32_t ck = c + uint32_t(k) * gridDim.x;
@@ -391,7 +406,7 @@ __global__ void __launch_bounds__(kStagedThreads)
       const uint32_t cn = c + uint32_t(kStagedStages) * gridDim.x;
       if (cn < nchunks)
         bulk_load(stage[s], packed + uint64_t(cn) * kStagedBytes,
-                  chunk_bytes(cn), &bar[s]);
+                  chunk_bytes(cn), ctl.shortfall, &bar[s]);
     }
   }
 }
@@ -407,7 +422,7 @@ template <int ND>
 __global__ void __launch_bounds__(kStagedThreads)
     k_pack_staged(const char *__restrict__ strided, char *__restrict__ packed,
                   const __grid_constant__ Geometry g, uint32_t nchunks,
-                  uint64_t total_bytes) {
+                  uint64_t total_bytes, StagedCtl ctl) {
   __shared__ __align__(128) char stage[kStagedStages][kStagedBytes];
   __shared__ __align__(8) uint64_t bar[kStagedStages];
   __shared__ int gave_up;
@@ -424,7 +439,7 @@ __global__ void __launch_bounds__(kStagedThreads)
     if (lane == 0)
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::
                        "r"(smem_u32(&bar[s])),
-                   "r"(n)
+                   "r"(n + ctl.shortfall)
                    : "memory");
     __syncwarp();
     const uint32_t row0 = uint32_t(p0 / block);
@@ -467,7 +482,7 @@ __global__ void __launch_bounds__(kStagedThreads)
     __syncthreads();
     if (gave_up) {
       if (threadIdx.x == 0) {
-        atomicAdd(&g_staged_timeouts, 1);
+        staged_give_up(ctl);
         for (int k = 1; k < kStagedStages; ++k) {
           const uint32_t ck = c + uint32_t(k) * gridDim.x;
           if (ck < nchunks)
@@ -491,9 +506,10 @@ __global__ void __launch_bounds__(kStagedThreads)
   }
 }
 
-using StagedFn = void (*)(char *, const char *, Geometry, uint32_t, uint64_t);
+using StagedFn = void (*)(char *, const char *, Geometry, uint32_t, uint64_t,
+                          StagedCtl);
 using StagedPackFn = void (*)(const char *, char *, Geometry, uint32_t,
-                              uint64_t);
+                              uint64_t, StagedCtl);
 
 StagedPackFn pick_staged_pack(uint32_t nd) {
   switch (nd) {
@@ -506,13 +522,60 @@ StagedPackFn pick_staged_pack(uint32_t nd) {
   }
 }
 
-int64_t staged_timeouts() {
-  int v = 0;
-  if (cudaMemcpyFromSymbol(&v, g_staged_timeouts, sizeof(v)) != cudaSuccess) {
+// The failure word of the staged kernels: one int of mapped pinned host
+// memory (portable to every device), allocated at the first staged launch
+// outside a stream capture.  Until it exists the plain kernels run instead.
+namespace {
+std::once_flag g_fail_once;
+int *g_fail_host = nullptr, *g_fail_dev = nullptr;
+std::atomic<int64_t> g_fail_count{0};
+} // namespace
+
+static bool staged_channel(cudaStream_t stream) {
+  if (g_fail_dev)
+    return true;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
     cudaGetLastError();
-    return -1;
+    return false;
   }
-  return v;
+  if (cs != cudaStreamCaptureStatusNone)
+    return false;
+  std::call_once(g_fail_once, [] {
+    void *h = nullptr, *d = nullptr;
+    if (cudaHostAlloc(&h, 64, cudaHostAllocMapped | cudaHostAllocPortable) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFreeHost(h);
+      return;
+    }
+    *static_cast<volatile int *>(h) = 0;
+    g_fail_host = static_cast<int *>(h);
+    g_fail_dev = static_cast<int *>(d);
+  });
+  return g_fail_dev != nullptr;
+}
+
+bool staged_failed() {
+  if (!g_fail_host)
+    return false;
+  volatile int *f = g_fail_host;
+  if (*f == 0)
+    return false;
+  *f = 0;
+  g_fail_count++;
+  return true;
+}
+
+int64_t staged_timeouts() {
+  int64_t n = g_fail_count.load();
+  if (g_fail_host && *static_cast<volatile int *>(g_fail_host))
+    ++n;
+  return n;
 }
 
 template <int W> StagedFn pick_staged_nd(uint32_t nd) {
@@ -725,7 +788,8 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
   // needs a 16-B aligned packed base and a packed size that is a multiple of
   // 16 bytes; pack needs every row piece 16-B aligned on both sides (width
   // 16).  Both sides must be device memory proper: host-mapped and managed
-  // buffers take the plain kernels.
+  // buffers take the plain kernels; so do launches before the failure word
+  // exists (see staged_channel).
   const uint64_t bytes = uint64_t(g.rows) * uint64_t(g.block);
   const bool wide = g.width == 16 && bytes >= (uint64_t(32) << 20);
   const bool narrow_unpack =
@@ -734,7 +798,8 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
       bytes % 16 == 0 &&
       (unpack ? (reinterpret_cast<uintptr_t>(packed) & 15) == 0
               : g.width == 16) &&
-      classify(strided).is_device && classify(packed).is_device) {
+      classify(strided).is_device && classify(packed).is_device &&
+      staged_channel(stream)) {
     const uint32_t nchunks =
         uint32_t((bytes + kStagedBytes - 1) / kStagedBytes);
     // measured on the strided sweep: 3 CTAs per SM for long aligned
@@ -744,12 +809,13 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
                         : wide ? 3 : 8;
     const uint32_t blocks = std::max<uint32_t>(
         1, std::min<uint32_t>(nchunks, uint32_t(sms) * uint32_t(bps)));
+    const StagedCtl ctl{g_fail_dev, uint32_t(env().staged_shortfall)};
     if (unpack)
       pick_staged(g.width, g.nd)<<<blocks, kStagedThreads, 0, stream>>>(
-          const_cast<char *>(strided), packed, g, nchunks, bytes);
+          const_cast<char *>(strided), packed, g, nchunks, bytes, ctl);
     else
       pick_staged_pack(g.nd)<<<blocks, kStagedThreads, 0, stream>>>(
-          strided, packed, g, nchunks, bytes);
+          strided, packed, g, nchunks, bytes, ctl);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
       return cuda_error(e, "staged kernel launch");
@@ -842,4 +908,12 @@ extern "C" int tempi_unpack(const tempi_desc *d, const void *packed,
   return launch_geometry(g, base, const_cast<char *>(
                                       static_cast<const char *>(packed)),
                          true, cfg, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int tempi_staged_check(void) {
+  if (staged_failed())
+    return set_error(TEMPI_ERR_TIMEOUT,
+                     "a staged pack/unpack kernel gave up waiting on its bulk "
+                     "copies; its output is incomplete");
+  return TEMPI_OK;
 }

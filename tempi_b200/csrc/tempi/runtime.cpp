@@ -5,6 +5,8 @@
 
 #include <nvtx3/nvToolsExtCudaRt.h>
 
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -50,6 +52,8 @@ void read_env() {
     e.wait_timeout_s = std::atof(s);
   if (const char *s = std::getenv("TEMPI_HOST_LINK"))
     e.host_link_dma = std::string(s) != "kernel";
+  if (const char *s = std::getenv("TEMPI_TEST_STAGED_SHORTFALL"))
+    e.staged_shortfall = std::max(0, std::min(4096, std::atoi(s))) & ~15;
   if (const char *cd = std::getenv("TEMPI_CACHE_DIR")) {
     e.cache_dir = cd;
   } else if (const char *x = std::getenv("XDG_CACHE_HOME")) {

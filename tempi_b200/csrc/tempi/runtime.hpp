@@ -29,6 +29,11 @@ struct Env {
   // TEMPI_HOST_LINK=kernel: contiguous runs between pinned host buffers go
   // through the kernels too, instead of the copy-engine pipeline
   bool host_link_dma = true;
+  // TEMPI_TEST_STAGED_SHORTFALL=<bytes>: the staged kernels' barriers expect
+  // that many bytes per chunk beyond what their copies deliver, so every
+  // bounded wait runs out (about a second) and the give-up path reports a
+  // timeout.  For tests of that path only; 0 (the default) in normal use.
+  int staged_shortfall = 0;
 };
 const Env &env();
 void read_env(); // re-read the environment (MPI_Init does this)

@@ -40,7 +40,8 @@ int to_mpi(int tempi_err) {
 
 int sync(cudaStream_t s) {
   cudaError_t e = cudaStreamSynchronize(s);
-  return e == cudaSuccess ? TEMPI_OK : cuda_error(e, "stream synchronize");
+  return e == cudaSuccess ? tempi_staged_check()
+                          : cuda_error(e, "stream synchronize");
 }
 
 void *host_dev_ptr(void *h) {
@@ -295,6 +296,10 @@ public:
       err = to_mpi(cuda_error(e, "isend pack"));
       return err;
     }
+    if (int c = tempi_staged_check()) {
+      err = to_mpi(c);
+      return err;
+    }
     started_ = true;
     err = libmpi.Start(&req_);
     return err;
@@ -388,6 +393,8 @@ public:
     cudaError_t e = cudaEventSynchronize(ev_);
     if (e != cudaSuccess)
       return to_mpi(cuda_error(e, "irecv unpack"));
+    if (int c = tempi_staged_check())
+      return to_mpi(c);
     if (status)
       *status = st_;
     return MPI_SUCCESS;

@@ -592,3 +592,65 @@ def test_staged_pack_matches_oracle(cuda, mpi_init):
             assert got[:want.size].tobytes() == want.tobytes(), (d.block, incount, bps)
             assert (got[want.size:] == 0x5A).all(), (d.block, incount, bps)
     assert _lib.counter("staged_timeouts") == before == 0
+    assert _lib.tempi().tempi_staged_check() == 0
+
+
+def test_staged_give_up_is_reported(cuda, mpi_init):
+    """A staged kernel whose bounded waits run out must not pass for a good
+    copy.  TEMPI_TEST_STAGED_SHORTFALL makes every chunk's barrier expect 16
+    bytes more than its bulk copy delivers, so each wait gives up after about
+    a second: tempi_staged_check then reports TEMPI_ERR_TIMEOUT (once), the
+    counter moves, and the interposed MPI_Unpack returns an error instead of
+    MPI_SUCCESS.  With the knob cleared the same calls copy correctly again
+    on the same context."""
+    import os
+
+    import torch
+
+    from tests.test_canon import desc_pack
+
+    lib = _lib.tempi()
+    # 1 MiB packed, rows of 256 B: 128 chunks, one per CTA, so each CTA
+    # waits once and has no other copies to drain
+    d = _lib.Desc.make(0, 1 << 22, 256, [4096], [1024])
+    span = d.block + d.strides[0] * (d.counts[0] - 1)
+    src_np = H.splitmix_bytes(span, 77)
+    want = desc_pack(d, src_np, 1)
+    packed = torch.from_numpy(want).cuda()
+    exp = np.full(span, 0xAA, np.uint8)
+    T.unpack(T.hvector(4096, 256, 1024, T.BYTE), want, exp, 1)
+    cfg = _lib.Config(4, 0, 256, 0, 8, 0)
+    t = mpi.Type_create_hvector(4096, 256, 1024, mpi.BYTE)
+    assert mpi.Type_commit(t) == 0
+    before = _lib.counter("staged_timeouts")
+    assert lib.tempi_staged_check() == 0
+    os.environ["TEMPI_TEST_STAGED_SHORTFALL"] = "16"
+    os.environ["TEMPI_DISPATCH"] = "heuristic"  # fixed rules: staged for this unpack
+    try:
+        lib.tempi_reload_env()
+        dst = torch.full((span,), 0xAA, dtype=torch.uint8, device="cuda")
+        _lib.check(lib.tempi_unpack(ctypes.byref(d), packed.data_ptr(), 1, dst.data_ptr(),
+                                    ctypes.byref(cfg), None))
+        sync()
+        assert lib.tempi_last_kernel().decode().startswith("staged")
+        assert lib.tempi_staged_check() == 4  # TEMPI_ERR_TIMEOUT
+        assert lib.tempi_staged_check() == 0  # reported once
+        assert _lib.counter("staged_timeouts") == before + 1
+        err, _ = mpi.Unpack(packed.data_ptr(), want.size, dst.data_ptr(), 1, t)
+        assert err != 0
+        assert lib.tempi_last_kernel().decode().startswith("staged")
+        assert _lib.counter("staged_timeouts") == before + 2
+    finally:
+        del os.environ["TEMPI_TEST_STAGED_SHORTFALL"]
+        del os.environ["TEMPI_DISPATCH"]
+        lib.tempi_reload_env()
+    dst = torch.full((span,), 0xAA, dtype=torch.uint8, device="cuda")
+    _lib.check(lib.tempi_unpack(ctypes.byref(d), packed.data_ptr(), 1, dst.data_ptr(),
+                                ctypes.byref(cfg), None))
+    sync()
+    assert lib.tempi_staged_check() == 0
+    assert host(dst).tobytes() == exp.tobytes()
+    err, _ = mpi.Unpack(packed.data_ptr(), want.size, dst.data_ptr(), 1, t)
+    assert err == 0 and host(dst).tobytes() == exp.tobytes()
+    assert _lib.counter("staged_timeouts") == before + 2
+    mpi.Type_free(t)
