@@ -527,12 +527,14 @@ StagedPackFn pick_staged_pack(uint32_t nd) {
 // outside a stream capture.  Until it exists the plain kernels run instead.
 namespace {
 std::once_flag g_fail_once;
+// written once inside g_fail_once, then published by g_fail_ready
 int *g_fail_host = nullptr, *g_fail_dev = nullptr;
+std::atomic<bool> g_fail_ready{false};
 std::atomic<int64_t> g_fail_count{0};
 } // namespace
 
 static bool staged_channel(cudaStream_t stream) {
-  if (g_fail_dev)
+  if (g_fail_ready.load(std::memory_order_acquire))
     return true;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
@@ -556,24 +558,25 @@ static bool staged_channel(cudaStream_t stream) {
     *static_cast<volatile int *>(h) = 0;
     g_fail_host = static_cast<int *>(h);
     g_fail_dev = static_cast<int *>(d);
+    g_fail_ready.store(true, std::memory_order_release);
   });
-  return g_fail_dev != nullptr;
+  return g_fail_ready.load(std::memory_order_acquire);
 }
 
 bool staged_failed() {
-  if (!g_fail_host)
+  if (!g_fail_ready.load(std::memory_order_acquire))
     return false;
-  volatile int *f = g_fail_host;
-  if (*f == 0)
+  // one reader takes the word, so two threads never report one failure twice
+  if (__atomic_exchange_n(g_fail_host, 0, __ATOMIC_ACQ_REL) == 0)
     return false;
-  *f = 0;
   g_fail_count++;
   return true;
 }
 
 int64_t staged_timeouts() {
   int64_t n = g_fail_count.load();
-  if (g_fail_host && *static_cast<volatile int *>(g_fail_host))
+  if (g_fail_ready.load(std::memory_order_acquire) &&
+      *static_cast<volatile int *>(g_fail_host))
     ++n;
   return n;
 }
