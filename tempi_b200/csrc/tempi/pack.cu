@@ -22,6 +22,11 @@
 //  * k_rows: one warp per row, lanes stride across the row's words, U loads
 //    in flight per lane; the row offset is computed once per row.  Used for
 //    wide rows.
+//  * k_rows_shift: a group of lanes per row, 16-B words realigned by funnel
+//    shifts, for rows whose two sides disagree modulo 16.
+//  * k_pack_staged / k_unpack_staged: 8 KB chunks of the packed stream move
+//    between global and shared memory by bulk asynchronous copies counted on
+//    mbarriers (bounded waits), the other side by coalesced plain accesses.
 //  * grids are a multiple of the SM count and grid-stride over the work.
 
 #include "internal.hpp"
