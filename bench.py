@@ -586,8 +586,9 @@ def e2e_zero_copy(torch, sw, steps, warmup):
             "kernel_calls_per_step": round((kernels) / (steps + warmup), 1),
             "copy_engine_calls_per_step": round(dma / (steps + warmup), 1),
             "how": "MPI_Pack/MPI_Unpack on pinned host buffers: strided objects by kernels "
-                   "that read and write host memory directly, contiguous runs of 8 MiB or "
-                   "more by the copy-engine pipeline (link bytes = described bytes)"}
+                   "that read and write host memory directly; objects of 8 MiB or more that "
+                   "are one contiguous run, or rows of 128 B or more of one strided "
+                   "dimension, by the copy-engine pipeline (link bytes = described bytes)"}
 
 
 def sendrecv_bench(torch, mpi, reps=2):

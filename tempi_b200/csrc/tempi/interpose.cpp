@@ -35,15 +35,20 @@ int to_mpi(int e) {
   }
 }
 
-// Both buffers pinned host memory and the objects one contiguous run: the
-// copy engines move it across the host link (hostlink.cpp).
-bool use_host_link(const PtrInfo &a, const PtrInfo &b, const tempi_desc &d,
-                   int64_t count) {
+// Both buffers pinned host memory and enough bytes: the copy engines move
+// the objects across the host link (hostlink.cpp) when they are one
+// contiguous run (RUN) or rows of one strided dimension (ROWS, shape in
+// *rows); anything else stays on the kernels (NONE).
+enum class HostLink { NONE, RUN, ROWS };
+HostLink use_host_link(const PtrInfo &a, const PtrInfo &b, const tempi_desc &d,
+                       int64_t count, HostRows *rows) {
   if (!env().host_link_dma || !a.is_host || !b.is_host)
-    return false;
+    return HostLink::NONE;
   if (int64_t(count) * d.size < kHostLinkMinBytes)
-    return false;
-  return contiguous_run(d, count) == int64_t(count) * d.size;
+    return HostLink::NONE;
+  if (contiguous_run(d, count) == int64_t(count) * d.size)
+    return HostLink::RUN;
+  return host_rows(d, count, rows) ? HostLink::ROWS : HostLink::NONE;
 }
 
 // A contiguous device buffer goes through host staging under
@@ -156,10 +161,16 @@ int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
     return MPI_ERR_TRUNCATE;
   cudaStream_t s = pack_stream();
   int e;
-  if (use_host_link(in, out, r->desc, incount)) {
+  HostRows hr{};
+  const HostLink link = use_host_link(in, out, r->desc, incount, &hr);
+  if (link == HostLink::RUN) {
     e = host_link_copy(static_cast<char *>(outbuf) + *position,
                        static_cast<const char *>(inbuf) + r->desc.start,
                        size_t(bytes), s);
+  } else if (link == HostLink::ROWS) {
+    e = host_link_rows(static_cast<char *>(outbuf) + *position, hr.width,
+                       static_cast<const char *>(inbuf) + r->desc.start,
+                       hr.pitch, hr.width, hr.rows, s);
   } else {
     tempi_config cfg =
         choose_config(*r, incount, in.is_host, out.is_host, false);
@@ -206,10 +217,16 @@ int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
     return MPI_ERR_TRUNCATE;
   cudaStream_t s = pack_stream();
   int e;
-  if (use_host_link(in, out, r->desc, outcount)) {
+  HostRows hr{};
+  const HostLink link = use_host_link(in, out, r->desc, outcount, &hr);
+  if (link == HostLink::RUN) {
     e = host_link_copy(static_cast<char *>(outbuf) + r->desc.start,
                        static_cast<const char *>(inbuf) + *position,
                        size_t(bytes), s);
+  } else if (link == HostLink::ROWS) {
+    e = host_link_rows(static_cast<char *>(outbuf) + r->desc.start, hr.pitch,
+                       static_cast<const char *>(inbuf) + *position, hr.width,
+                       hr.width, hr.rows, s);
   } else {
     tempi_config cfg =
         choose_config(*r, outcount, out.is_host, in.is_host, true);

@@ -225,6 +225,68 @@ def test_host_to_host_contiguous_run(cuda, mpi_init, path, shape):
         _lib.tempi().tempi_reload_env()
 
 
+@pytest.mark.parametrize("path", ["dma", "kernel"])
+@pytest.mark.parametrize("shape", ["rows256_odd", "rows1000", "rows64_odd", "two_dims"])
+def test_host_to_host_strided_rows(cuda, mpi_init, path, shape):
+    """Pinned host typed and packed buffers with objects whose bytes are rows
+    of one strided dimension: the copy-engine 2-D path (rows of 128 B or
+    more, TEMPI_HOST_LINK unset) and the kernels write the oracle's bytes at
+    an odd packed position, and the unpack writes only the rows.  Rows of
+    64 B, and a layout with two strided dimensions, stay on the kernels
+    either way."""
+    import os
+
+    import torch
+
+    if shape == "rows256_odd":  # 3-D subarray of floats, 256-B rows at byte 28
+        ty = H.subarray([256, 256, 256], [256, 256, 64], [0, 0, 7], mpi.ORDER_C,
+                        H.named("FLOAT")).commit()
+        count, rows = 1, True
+    elif shape == "rows1000":  # 1000-B rows at 1040 B, 3 objects continuing the rows
+        ty = H.resized(H.hvector(3000, 1000, 1040, H.named("BYTE")), 0, 3000 * 1040).commit()
+        count, rows = 3, True
+    elif shape == "rows64_odd":  # 64-B rows at byte 120: below the 2-D path's row width
+        ty = H.subarray([256, 256, 256], [256, 256, 16], [0, 0, 30], mpi.ORDER_C,
+                        H.named("FLOAT")).commit()
+        count, rows = 2, False
+    else:  # a column block of a 2-D subarray repeated with a gap: two dimensions
+        ty = H.resized(H.subarray([2048, 2048], [2000, 512], [3, 7], mpi.ORDER_C,
+                                  H.named("FLOAT")), 0, 2048 * 2048 * 4 + 4096).commit()
+        count, rows = 3, False
+    assert ty.o.size * count >= 8 << 20
+    old = os.environ.get("TEMPI_HOST_LINK")
+    if path == "kernel":
+        os.environ["TEMPI_HOST_LINK"] = "kernel"
+    else:
+        os.environ.pop("TEMPI_HOST_LINK", None)
+    _lib.tempi().tempi_reload_env()
+    try:
+        src_np = H.splitmix_bytes(ty.o.extent * count + 64, 23)
+        src = torch.from_numpy(src_np).pin_memory()
+        pos0 = 7
+        packed = torch.zeros(ty.o.size * count + pos0 + 5, dtype=torch.uint8).pin_memory()
+        n0 = _lib.counter("host_link_copies")
+        err, pos = mpi.Pack(src.data_ptr(), count, ty.h, packed.data_ptr(), packed.numel(), pos0)
+        assert err == 0 and pos == pos0 + ty.o.size * count
+        want = T.pack(ty.o, src_np, count)
+        assert packed.numpy()[pos0:pos].tobytes() == want.tobytes()
+        assert not packed.numpy()[:pos0].any() and not packed.numpy()[pos:].any()
+        back = torch.full_like(src, 0xAA).pin_memory()
+        err, upos = mpi.Unpack(packed.data_ptr(), packed.numel(), back.data_ptr(), count, ty.h, pos0)
+        assert err == 0 and upos == pos
+        exp = np.full_like(src_np, 0xAA)
+        T.unpack(ty.o, want, exp, count)
+        assert back.numpy().tobytes() == exp.tobytes()
+        used = _lib.counter("host_link_copies") - n0
+        assert used == (2 if path == "dma" and rows else 0)
+    finally:
+        if old is None:
+            os.environ.pop("TEMPI_HOST_LINK", None)
+        else:
+            os.environ["TEMPI_HOST_LINK"] = old
+        _lib.tempi().tempi_reload_env()
+
+
 @pytest.mark.parametrize("where", ["host_host", "host_dev", "dev_host"])
 def test_every_configuration_on_host_memory(cuda, mpi_init, where):
     """Every kernel configuration the dispatcher can pick (word kernel at 3
