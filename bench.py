@@ -480,6 +480,9 @@ def driver():
         _lib.tempi()
         _driver = ctypes.CDLL(os.path.join(ROOT, "tempi_b200", "csrc", "libtempi_bench.so"))
         _driver.tempi_bench_flush.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        sz = ctypes.c_size_t
+        _driver.tempi_bench_copy2d.argtypes = [ctypes.c_void_p, sz, ctypes.c_void_p, sz, sz, sz,
+                                               ctypes.c_int, ctypes.c_void_p]
         _driver.tempi_bench_mpi_ops.argtypes = [
             ctypes.POINTER(BenchOp), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
             ctypes.c_size_t, ctypes.POINTER(ctypes.c_float)]
@@ -587,8 +590,9 @@ def e2e_zero_copy(torch, sw, steps, warmup):
             "copy_engine_calls_per_step": round(dma / (steps + warmup), 1),
             "how": "MPI_Pack/MPI_Unpack on pinned host buffers: strided objects by kernels "
                    "that read and write host memory directly; objects of 8 MiB or more that "
-                   "are one contiguous run, or rows of 128 B or more of one strided "
-                   "dimension, by the copy-engine pipeline (link bytes = described bytes)"}
+                   "are one contiguous run, and unpacks of rows of 128 B or more of one "
+                   "strided dimension, by the copy-engine pipeline (link bytes = described "
+                   "bytes)"}
 
 
 def sendrecv_bench(torch, mpi, reps=2):
@@ -1020,7 +1024,56 @@ def run_host_link(args):
     out["mpi_pack_host_to_host_each_way"] = gbs(pipeline, n)
     out["mpi_pack_used_copy_engines"] = _lib.counter("host_link_copies") > dma0
     assert torch.equal(ha, hb)
-    print(json.dumps({"host_link_gbs_per_direction": out, "bytes": n}))
+
+    # rows of one strided dimension: a lone 2-D copy each way, and MPI_Pack /
+    # MPI_Unpack host -> host by the copy-engine pipeline and by the kernels
+    rows_out = []
+    for width, pitch, off in ((64, 1024, 0), (64, 1024, 120), (256, 1024, 28),
+                              (1024, 4096, 116)):
+        nrows = (16 << 20) // width
+        assert off + (nrows - 1) * pitch + width <= n
+        src = ha.data_ptr() + off
+
+        def g2d():
+            _lib_check2d(driver().tempi_bench_copy2d(da.data_ptr(), width, src, pitch, width,
+                                                     nrows, 0, st.cuda_stream))
+
+        def s2d():
+            _lib_check2d(driver().tempi_bench_copy2d(hb.data_ptr() + off, pitch, da.data_ptr(),
+                                                     width, width, nrows, 1, st.cuda_stream))
+
+        ty = mpi.Type_create_hvector(nrows, width, pitch, mpi.BYTE)
+        assert mpi.Type_commit(ty) == 0
+        row = {"row_bytes": width, "pitch": pitch, "offset": off, "rows": nrows,
+               "copy2d_gather_h2d": gbs(g2d, width * nrows),
+               "copy2d_scatter_d2h": gbs(s2d, width * nrows)}
+        for path in ("copy_engines", "kernels"):
+            if path == "kernels":
+                os.environ["TEMPI_HOST_LINK"] = "kernel"
+            lib.tempi_reload_env()
+
+            def pk():
+                err, _ = mpi.Pack(src, 1, ty, hb.data_ptr(), n)
+                assert err == 0
+
+            def up():
+                err, _ = mpi.Unpack(hb.data_ptr(), n, db_host_ptr + off, 1, ty)
+                assert err == 0
+
+            db_host_ptr = ha.data_ptr()  # unpack back into the source span: same bytes
+            row[f"mpi_pack_{path}"] = gbs(pk, width * nrows)
+            row[f"mpi_unpack_{path}"] = gbs(up, width * nrows)
+            os.environ.pop("TEMPI_HOST_LINK", None)
+            lib.tempi_reload_env()
+        mpi.Type_free(ty)
+        rows_out.append(row)
+    print(json.dumps({"host_link_gbs_per_direction": out, "bytes": n,
+                      "strided_rows_gbs_per_direction": rows_out}))
+
+
+def _lib_check2d(rc):
+    if rc:
+        raise RuntimeError("cudaMemcpy2DAsync failed")
 
 
 def main():

@@ -48,6 +48,22 @@ typedef struct tempi_bench_op {
 // Evict the L2: write `bytes` of `buf`, then read them back so that the
 // lines left behind are clean (a dirty L2 would bill its write-back to the
 // next timed kernel).
+// One copy-engine 2-D copy of `height` rows of `width` bytes (cudaMemcpy2DAsync)
+// on `stream`: to_host != 0 copies device -> host, else host -> device.  For
+// the host-link measurements of 2-D copies.
+int tempi_bench_copy2d(void *dst, size_t dpitch, const void *src, size_t spitch,
+                       size_t width, size_t height, int to_host, void *stream) {
+  cudaError_t e = cudaMemcpy2DAsync(
+      dst, dpitch, src, spitch, width, height,
+      to_host ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice,
+      static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 2;
+  }
+  return 0;
+}
+
 int tempi_bench_flush(void *buf, size_t bytes, void *stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (!g_sink && cudaMalloc(&g_sink, sizeof(unsigned)) != cudaSuccess)

@@ -97,11 +97,12 @@ constexpr int64_t kHostLinkMinBytes = int64_t(8) << 20;
 // staging with the copy engines, both link directions busy at once; enqueued
 // on `s` and on link_stream(), and synchronised before it returns.
 int host_link_copy(void *dst, const void *src, size_t n, cudaStream_t s);
-// Narrowest row worth the 2-D copy-engine pipeline.  Measured on the sweep's
-// host-to-host points: 256-B rows at byte 28 unpack in 2.61 ms instead of
-// 3.25 ms by the kernels, 1-KiB rows gain 2-7 %, while 64-B rows at byte 120
-// unpack slower (1.52 against 1.33 ms) although a lone 2-D copy of them runs
-// at 24 GB/s: in the pipeline the two directions overlap poorly.
+// Narrowest row worth the 2-D copy-engine pipeline (used for unpacks).
+// Measured on the sweep's host-to-host points: 256-B rows at byte 28 unpack
+// in 2.61 ms instead of 3.25 ms by the kernels, 1-KiB rows gain 2-7 %, while
+// 64-B rows at byte 120 unpack slower (1.52 against 1.33 ms) although a lone
+// 2-D copy of them runs at 14-18 GB/s: in the pipeline the two directions
+// overlap poorly.
 constexpr int64_t kHostLinkMinRow = 128;
 // `incount` objects of `d` as `rows` rows of `width` bytes at `pitch`, when
 // they have exactly one strided dimension with rows of kHostLinkMinRow bytes
