@@ -114,9 +114,20 @@ int make_geometry(const tempi_desc *d, int64_t incount, uintptr_t strided_base,
                   uintptr_t packed_base, int max_width, Geometry *g,
                   bool *empty);
 
-// Launch one pack (unpack=false) or unpack on `stream`.
+// Launch one pack (unpack=false) or unpack on `stream`.  both_device: 1 when
+// the caller knows both buffers are device memory proper, 0 when it knows
+// they are not, -1 to ask the runtime (only the staged kernels need it).
 int launch_geometry(const Geometry &g, const char *strided_base, char *packed,
-                    bool unpack, const tempi_config *cfg, cudaStream_t stream);
+                    bool unpack, const tempi_config *cfg, cudaStream_t stream,
+                    int both_device = -1);
+// tempi_pack / tempi_unpack with the buffers' kind already known (see
+// launch_geometry's both_device).
+int pack_known(const tempi_desc *d, const void *origin, int64_t incount,
+               void *packed, const tempi_config *cfg, cudaStream_t stream,
+               int both_device);
+int unpack_known(const tempi_desc *d, const void *packed, int64_t incount,
+                 void *origin, const tempi_config *cfg, cudaStream_t stream,
+                 int both_device);
 
 int num_sms();
 // Staged launches (kernel 4) that gave up waiting on a bulk copy, counted

@@ -172,8 +172,9 @@ int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
   } else {
     tempi_config cfg =
         choose_config(*r, incount, in.is_host, out.is_host, false);
-    e = tempi_pack(&r->desc, in.device_ptr, incount,
-                   static_cast<char *>(out.device_ptr) + *position, &cfg, s);
+    e = pack_known(&r->desc, in.device_ptr, incount,
+                   static_cast<char *>(out.device_ptr) + *position, &cfg, s,
+                   in.is_device && out.is_device ? 1 : 0);
   }
   if (!e) {
     cudaError_t ce = cudaStreamSynchronize(s);
@@ -228,9 +229,10 @@ int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
   } else {
     tempi_config cfg =
         choose_config(*r, outcount, out.is_host, in.is_host, true);
-    e = tempi_unpack(&r->desc,
+    e = unpack_known(&r->desc,
                      static_cast<const char *>(in.device_ptr) + *position,
-                     outcount, out.device_ptr, &cfg, s);
+                     outcount, out.device_ptr, &cfg, s,
+                     in.is_device && out.is_device ? 1 : 0);
   }
   if (!e) {
     cudaError_t ce = cudaStreamSynchronize(s);

@@ -788,8 +788,8 @@ int make_geometry(const tempi_desc *d, int64_t incount, uintptr_t sbase,
 }
 
 int launch_geometry(const Geometry &g, const char *strided, char *packed,
-                    bool unpack, const tempi_config *cfg,
-                    cudaStream_t stream) {
+                    bool unpack, const tempi_config *cfg, cudaStream_t stream,
+                    int both_device) {
   const int sms = num_sms();
   int kernel = cfg ? cfg->kernel : 0;
   // the staged kernels (4), where their bulk copies are allowed: unpack
@@ -806,7 +806,9 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
       bytes % 16 == 0 &&
       (unpack ? (reinterpret_cast<uintptr_t>(packed) & 15) == 0
               : g.width == 16) &&
-      classify(strided).is_device && classify(packed).is_device &&
+      (both_device >= 0
+           ? both_device == 1
+           : classify(strided).is_device && classify(packed).is_device) &&
       staged_channel(stream)) {
     const uint32_t nchunks =
         uint32_t((bytes + kStagedBytes - 1) / kStagedBytes);
@@ -877,13 +879,9 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
   return TEMPI_OK;
 }
 
-} // namespace tempi
-
-using namespace tempi;
-
-extern "C" int tempi_pack(const tempi_desc *d, const void *origin,
-                          int64_t incount, void *packed,
-                          const tempi_config *cfg, void *stream) {
+int pack_known(const tempi_desc *d, const void *origin, int64_t incount,
+               void *packed, const tempi_config *cfg, cudaStream_t stream,
+               int both_device) {
   if (!d)
     return set_error(TEMPI_ERR_ARG, "null descriptor");
   const char *base = static_cast<const char *>(origin) + d->start;
@@ -896,12 +894,12 @@ extern "C" int tempi_pack(const tempi_desc *d, const void *origin,
   counters().packs++;
   counters().pack_bytes += int64_t(g.rows) * g.block;
   return launch_geometry(g, base, static_cast<char *>(packed), false, cfg,
-                         static_cast<cudaStream_t>(stream));
+                         stream, both_device);
 }
 
-extern "C" int tempi_unpack(const tempi_desc *d, const void *packed,
-                            int64_t incount, void *origin,
-                            const tempi_config *cfg, void *stream) {
+int unpack_known(const tempi_desc *d, const void *packed, int64_t incount,
+                 void *origin, const tempi_config *cfg, cudaStream_t stream,
+                 int both_device) {
   if (!d)
     return set_error(TEMPI_ERR_ARG, "null descriptor");
   char *base = static_cast<char *>(origin) + d->start;
@@ -913,9 +911,27 @@ extern "C" int tempi_unpack(const tempi_desc *d, const void *packed,
     return err;
   counters().unpacks++;
   counters().unpack_bytes += int64_t(g.rows) * g.block;
-  return launch_geometry(g, base, const_cast<char *>(
-                                      static_cast<const char *>(packed)),
-                         true, cfg, static_cast<cudaStream_t>(stream));
+  return launch_geometry(
+      g, base, const_cast<char *>(static_cast<const char *>(packed)), true,
+      cfg, stream, both_device);
+}
+
+} // namespace tempi
+
+using namespace tempi;
+
+extern "C" int tempi_pack(const tempi_desc *d, const void *origin,
+                          int64_t incount, void *packed,
+                          const tempi_config *cfg, void *stream) {
+  return pack_known(d, origin, incount, packed, cfg,
+                    static_cast<cudaStream_t>(stream), -1);
+}
+
+extern "C" int tempi_unpack(const tempi_desc *d, const void *packed,
+                            int64_t incount, void *origin,
+                            const tempi_config *cfg, void *stream) {
+  return unpack_known(d, packed, incount, origin, cfg,
+                      static_cast<cudaStream_t>(stream), -1);
 }
 
 extern "C" int tempi_staged_check(void) {
