@@ -133,6 +133,9 @@ int num_sms();
 // Staged launches (kernel 4) that gave up waiting on a bulk copy, counted
 // once the host has seen their failure word (0 unless something failed).
 int64_t staged_timeouts();
+// Allocate the staged kernels' failure word now (MPI_Init calls this with
+// stream 0), unless `stream` is being captured; whether it exists.
+bool staged_channel(cudaStream_t stream);
 // After synchronising the stream of a staged launch: whether a staged kernel
 // gave up since the last call (its output is then incomplete).  Clears the
 // failure word.

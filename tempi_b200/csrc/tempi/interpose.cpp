@@ -71,6 +71,10 @@ bool contiguous_staged(const TypeRecord *r, const PtrInfo &p, int count) {
 void on_init() {
   read_env();
   dispatch_init();
+  // the staged kernels' failure word, allocated here rather than at a first
+  // launch that might come while another thread captures a stream
+  if (!env().disable)
+    staged_channel(nullptr);
   // the named types a contiguous send uses are known from the start, as in
   // the reference's types_init (src/internal/types.cpp:723-755, called from
   // src/init.cpp:63 unless TEMPI is disabled)

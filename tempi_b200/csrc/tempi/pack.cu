@@ -528,8 +528,9 @@ StagedPackFn pick_staged_pack(uint32_t nd) {
 }
 
 // The failure word of the staged kernels: one int of mapped pinned host
-// memory (portable to every device), allocated at the first staged launch
-// outside a stream capture.  Until it exists the plain kernels run instead.
+// memory (portable to every device), allocated by MPI_Init, or else at the
+// first staged launch outside a stream capture.  Until it exists the plain
+// kernels run instead.
 namespace {
 std::once_flag g_fail_once;
 // written once inside g_fail_once, then published by g_fail_ready
@@ -538,7 +539,7 @@ std::atomic<bool> g_fail_ready{false};
 std::atomic<int64_t> g_fail_count{0};
 } // namespace
 
-static bool staged_channel(cudaStream_t stream) {
+bool staged_channel(cudaStream_t stream) {
   if (g_fail_ready.load(std::memory_order_acquire))
     return true;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
