@@ -183,6 +183,20 @@ def cpu_buffers(items, seed=7):
     return bufs
 
 
+def cpu_model():
+    """The host CPU's model name and logical core count."""
+    name = "unknown"
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    name = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": name, "nproc": os.cpu_count()}
+
+
 def cpu_baseline(budget_s=12.0):
     """Single-core C walker on the sweep with incount 1 per point, repeated
     for about `budget_s` seconds."""
@@ -197,7 +211,8 @@ def cpu_baseline(budget_s=12.0):
     dt = time.perf_counter() - t0
     return {"value": round(nbytes / dt / 1e9, 3), "unit": "GB/s", "cores": 1, "kind": "port",
             "sample": f"{reps} passes over the {len(items)} sweep points at incount 1 "
-                      f"({dt:.1f} s), pack + unpack, oracle/typemap.c single thread"}
+                      f"({dt:.1f} s), pack + unpack, oracle/typemap.c single thread",
+            "cpu": cpu_model()}
 
 
 def run_reference(args):
@@ -225,7 +240,8 @@ def run_reference(args):
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": nthreads,
                          "kind": "port",
                          "sample": "every sweep point at full incount per step, pack + unpack, "
-                                   "oracle/typemap.c on all host threads"},
+                                   "oracle/typemap.c on all host threads",
+                         "cpu": cpu_model()},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
