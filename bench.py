@@ -34,6 +34,10 @@ Also reported on the same GPU in the same run:
 
 --impl reference times that C walker with every host core on the same
 workload (the reference's path for host buffers is the library's MPI_Pack).
+
+Defaults: 50 warm-up steps, then 50 timed steps.  In a fresh process the
+first ~30 steps run about 6 % slower than every later one, so a warm-up of a
+few steps would time that transient instead of the steady state.
 """
 from __future__ import annotations
 
@@ -1095,8 +1099,11 @@ def _lib_check2d(rc):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    # defaults: the first ~30 steps of a fresh process run about 6 % slower
+    # than the steady state (a transient of the driver or GPU, not of this
+    # library's caches), so the default warm-up outlasts it
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
