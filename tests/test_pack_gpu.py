@@ -657,6 +657,64 @@ def test_staged_pack_matches_oracle(cuda, mpi_init):
     assert _lib.tempi().tempi_staged_check() == 0
 
 
+@pytest.mark.parametrize("kernel", [1, 2, 3])
+def test_plain_kernels_random_geometries(cuda, mpi_init, kernel):
+    """The word, row and shift kernels, forced, on 60 seeded random
+    non-overlapping descriptors (zero to four strided dimensions, one to five
+    objects, every alignment of block, start and packed offset, 128 to 512
+    threads, 4 to 32 lanes per row for the shift kernel): each pack equals the
+    descriptor oracle and each unpack writes exactly the described bytes."""
+    import torch
+
+    from tests.test_canon import desc_pack
+
+    rng = np.random.default_rng(900 + kernel)
+    lib = _lib.tempi()
+    for case in range(60):
+        nd = int(rng.integers(0, 5))
+        unit = int(rng.choice([1, 2, 4, 8, 16]))
+        block = unit * int(rng.integers(1, 120 if nd else 4000))
+        counts, strides, span = [], [], block
+        for k in range(nd):
+            c = int(rng.integers(2, 30))
+            st = span + int(rng.integers(0, 40))  # any alignment, past everything inside
+            counts.append(c)
+            strides.append(st)
+            span = st * (c - 1) + span
+        incount = int(rng.integers(1, 6))
+        extent = span + int(rng.integers(0, 24))
+        start = int(rng.integers(0, 24))
+        d = _lib.Desc.make(start, extent, block, counts, strides)
+        total = d.size * incount
+        if total == 0 or total > (1 << 20):
+            continue
+        nbytes = start + extent * (incount - 1) + span + 64
+        src_np = H.splitmix_bytes(nbytes, 3000 + case)
+        want = desc_pack(d, src_np, incount)
+        src = torch.from_numpy(src_np).cuda()
+        poff = int(rng.integers(0, 17))
+        threads = int(rng.choice([128, 256, 512])) if kernel != 3 else 256
+        lanes = int(rng.choice([4, 8, 16, 32])) if kernel == 3 else 0
+        cfg = _lib.Config(kernel, 0, threads, lanes, 0, 0)
+        packed = torch.full((total + poff + 64,), 0x5A, dtype=torch.uint8, device="cuda")
+        _lib.check(lib.tempi_pack(ctypes.byref(d), src.data_ptr(), incount,
+                                  packed.data_ptr() + poff, ctypes.byref(cfg), None))
+        sync()
+        got = host(packed)
+        assert got[poff:poff + total].tobytes() == want.tobytes(), (case, d.as_dict(), incount)
+        assert (got[:poff] == 0x5A).all() and (got[poff + total:] == 0x5A).all(), case
+        dst = torch.full((nbytes,), 0xAA, dtype=torch.uint8, device="cuda")
+        _lib.check(lib.tempi_unpack(ctypes.byref(d), packed.data_ptr() + poff, incount,
+                                    dst.data_ptr(), ctypes.byref(cfg), None))
+        sync()
+        exp = np.full(nbytes, 0xAA, np.uint8)
+        shape = [incount] + [d.counts[k] for k in reversed(range(d.ndims))] + [d.block]
+        strd = [d.extent] + [d.strides[k] for k in reversed(range(d.ndims))] + [1]
+        np.lib.stride_tricks.as_strided(exp[d.start:], shape=shape, strides=strd,
+                                        writeable=True)[...] = want.reshape(shape)
+        assert host(dst).tobytes() == exp.tobytes(), (case, d.as_dict(), incount)
+
+
 def test_staged_random_geometries(cuda, mpi_init):
     """The staged kernels (kernel 4) on 100 seeded random descriptors: zero to
     four strided dimensions that do not overlap, one to five objects, block
