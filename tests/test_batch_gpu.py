@@ -175,3 +175,55 @@ def test_batch_of_1500_regions(cuda, mpi_init):
     torch.cuda.synchronize()
     assert packed.cpu().numpy().tobytes() == np.concatenate(wants).tobytes()
     _lib.tempi().tempi_batch_destroy(h)
+
+
+@pytest.mark.parametrize("unpack", [0, 1])
+def test_batch_random_regions(cuda, mpi_init, unpack):
+    """One batched launch over 50 seeded random regions (0-3 strided
+    dimensions at any alignment, 1-3 objects each, some empty) packing into,
+    or unpacking from, one packed buffer at odd offsets: the packed bytes
+    equal each region's descriptor oracle in order, and an unpack writes
+    exactly the described bytes."""
+    import ctypes
+
+    import torch
+
+    from .test_canon import desc_pack
+    from .test_exchange_gpu import _rand_desc, desc_unpack
+
+    rng = np.random.default_rng(515 + unpack)
+    regs, pos, base = [], 0, 0
+    for i in range(50):
+        d = _rand_desc(rng, 100000)
+        n = 0 if i % 17 == 5 else int(rng.integers(1, 4))
+        pos += int(rng.integers(0, 8))
+        regs.append((base, d, n, pos))
+        pos += d.size * n
+        base += d.extent * max(n, 1) + 64
+    typed_np = H.splitmix_bytes(base, 99)
+    packed_np = H.splitmix_bytes(pos + 64, 98)
+    typed = torch.from_numpy(typed_np if not unpack else np.full(base, 0xAA, np.uint8)).cuda()
+    packed = torch.from_numpy(packed_np if unpack else np.full(pos + 64, 0x5A, np.uint8)).cuda()
+    arr = (_lib.Region * len(regs))()
+    for k, (b, d, n, off) in enumerate(regs):
+        arr[k].origin = typed.data_ptr() + b
+        arr[k].packed = packed.data_ptr() + off
+        arr[k].desc = d
+        arr[k].incount = n
+    h = ctypes.c_void_p()
+    _lib.check(_lib.tempi().tempi_batch_create(arr, len(regs), unpack, ctypes.byref(h)))
+    _lib.check(_lib.tempi().tempi_batch_launch(h, None))
+    torch.cuda.synchronize()
+    _lib.tempi().tempi_batch_destroy(h)
+    if not unpack:
+        want = np.full(pos + 64, 0x5A, np.uint8)
+        for b, d, n, off in regs:
+            if n:
+                want[off: off + d.size * n] = desc_pack(d, typed_np[b:], n)
+        assert packed.cpu().numpy().tobytes() == want.tobytes()
+    else:
+        want = np.full(base, 0xAA, np.uint8)
+        for b, d, n, off in regs:
+            if n:
+                desc_unpack(d, packed_np[off: off + d.size * n], want[b:], n)
+        assert typed.cpu().numpy().tobytes() == want.tobytes()

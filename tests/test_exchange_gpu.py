@@ -156,3 +156,66 @@ def test_alltoallw_mixed_edges_use_isir(cuda, mpi_init):
     T.unpack(st.o, T.pack(st.o, buf_np, 1, origin=1000), want, 1, origin=3000)
     assert out.cpu().numpy().tobytes() == want.tobytes()
     mpi.Comm_free(comm)
+
+
+def _rand_desc(rng, max_bytes):
+    """A seeded random non-overlapping descriptor of at most `max_bytes`
+    described bytes: 0-3 strided dimensions at any alignment."""
+    while True:
+        nd = int(rng.integers(0, 4))
+        block = int(rng.integers(1, 300 if nd else 5000))
+        counts, strides, span = [], [], block
+        for _ in range(nd):
+            c = int(rng.integers(1, 20))
+            st = span + int(rng.integers(0, 24))
+            counts.append(c)
+            strides.append(st)
+            span = st * (c - 1) + span
+        d = _lib.Desc.make(int(rng.integers(0, 20)), span + int(rng.integers(0, 20)),
+                           block, counts, strides)
+        if 0 < d.size <= max_bytes:
+            return d
+
+
+def test_copy_batch_random_pairs(cuda, mpi_init):
+    """One fused copy of 40 seeded random (source layout, destination layout)
+    pairs of equal byte counts -- the destination a row layout of a different
+    row length and alignment -- into one destination buffer: every pair's
+    bytes arrive in type-map order, and no other byte changes."""
+    import torch
+
+    rng = np.random.default_rng(31337)
+    srcs, dsts, pairs = [], [], []
+    sbase = dbase = 0
+    for i in range(40):
+        sd = _rand_desc(rng, 200000)
+        sc = int(rng.integers(1, 4))
+        total = sd.size * sc
+        divisors = [b for b in range(1, min(total, 4096) + 1) if total % b == 0]
+        bl = int(rng.choice(divisors))
+        cnt = total // bl
+        st = bl + int(rng.integers(0, 40))
+        dd = _lib.Desc.make(int(rng.integers(0, 16)), st * cnt + 16, bl, [cnt], [st])
+        srcs.append((sbase, sd, sc))
+        dsts.append((dbase, dd))
+        sbase += sd.extent * sc + 64
+        dbase += dd.extent + 64
+    src_np = H.splitmix_bytes(sbase, 4242)
+    dst_np = np.full(dbase, 0xAA, np.uint8)
+    src = torch.from_numpy(src_np).cuda()
+    dst = torch.from_numpy(dst_np.copy()).cuda()
+    arr = (_lib.CopyRegion * 40)()
+    for k, ((sb, sd, sc), (db, dd)) in enumerate(zip(srcs, dsts)):
+        r = arr[k]
+        r.src_origin, r.dst_origin = src.data_ptr() + sb, dst.data_ptr() + db
+        r.src_desc, r.dst_desc, r.src_count, r.dst_count = sd, dd, sc, 1
+    h = ctypes.c_void_p()
+    _lib.check(_lib.tempi().tempi_batch_create_copy(arr, 40, ctypes.byref(h)))
+    _lib.check(_lib.tempi().tempi_batch_launch(h, None))
+    torch.cuda.synchronize()
+    _lib.tempi().tempi_batch_destroy(h)
+    want = dst_np.copy()
+    for (sb, sd, sc), (db, dd) in zip(srcs, dsts):
+        seg = want[db: db + dd.extent + 64]
+        desc_unpack(dd, desc_pack(sd, src_np[sb: sb + sd.extent * sc + 64], sc), seg, 1)
+    assert dst.cpu().numpy().tobytes() == want.tobytes()
