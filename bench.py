@@ -1048,6 +1048,7 @@ def run_host_link(args):
     # rows of one strided dimension: a lone 2-D copy each way, and MPI_Pack /
     # MPI_Unpack host -> host by the copy-engine pipeline and by the kernels
     rows_out = []
+    saved = os.environ.get("TEMPI_HOST_LINK")
     for width, pitch, off in ((64, 1024, 0), (64, 1024, 120), (256, 1024, 28),
                               (1024, 4096, 116)):
         nrows = (16 << 20) // width
@@ -1070,6 +1071,8 @@ def run_host_link(args):
         for path in ("copy_engines", "kernels"):
             if path == "kernels":
                 os.environ["TEMPI_HOST_LINK"] = "kernel"
+            else:
+                os.environ.pop("TEMPI_HOST_LINK", None)
             lib.tempi_reload_env()
 
             def pk():
@@ -1084,6 +1087,8 @@ def run_host_link(args):
             row[f"mpi_pack_{path}"] = gbs(pk, width * nrows)
             row[f"mpi_unpack_{path}"] = gbs(up, width * nrows)
             os.environ.pop("TEMPI_HOST_LINK", None)
+            if saved is not None:
+                os.environ["TEMPI_HOST_LINK"] = saved
             lib.tempi_reload_env()
         mpi.Type_free(ty)
         rows_out.append(row)
