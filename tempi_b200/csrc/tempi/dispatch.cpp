@@ -6,11 +6,13 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <fstream>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace tempi {
@@ -40,7 +42,10 @@ struct Model {
   int members = 0;
   float y_mean[TEMPI_MLP_OUT], y_std[TEMPI_MLP_OUT];
   std::vector<float> params;
-  float *dev_params = nullptr, *dev_x = nullptr, *dev_out = nullptr;
+  float *dev_params = nullptr;
+  // one inference's input row and outputs, in mapped pinned host memory
+  // (the kernel reads and writes them over the link: no copies to wait for)
+  float *host_io = nullptr, *dev_io = nullptr;
   std::string source;
 };
 
@@ -52,6 +57,13 @@ struct Table {
 
 std::mutex g_mu;
 Model g_model;
+// Choices by layout, shared by every type handle with the same descriptor,
+// object count, buffer kinds, direction and policy, so committing a shape
+// again (a new handle for a layout seen before) costs no inference or
+// measurement.  Guarded by g_mu; cleared when a new model loads, and when it
+// grows past kMaxLayouts.
+std::unordered_map<std::string, int> g_layouts;
+constexpr size_t kMaxLayouts = size_t(1) << 16;
 Table g_table;
 int g_forced = -1;
 double g_spread_limit = 0.5; // log2 units: the members disagree by ~41 %
@@ -84,9 +96,10 @@ int load_model_file(const std::string &path) {
   m.source = path;
   std::lock_guard<std::mutex> l(g_mu);
   cudaFree(g_model.dev_params);
-  cudaFree(g_model.dev_x);
-  cudaFree(g_model.dev_out);
+  if (g_model.host_io)
+    cudaFreeHost(g_model.host_io);
   g_model = std::move(m);
+  g_layouts.clear(); // choices made with the previous model
   LOG_INFO("cost model loaded from %s (%d members)", path.c_str(),
            g_model.members);
   return TEMPI_OK;
@@ -135,34 +148,38 @@ int predict(const float f[TEMPI_MLP_IN], float mean[TEMPI_MLP_OUT],
   if (!m.loaded || !cuda_available())
     return TEMPI_ERR_UNSUPPORTED;
   cudaError_t e = cudaSuccess;
+  const size_t io_floats = TEMPI_MLP_IN + size_t(m.members) * TEMPI_MLP_OUT;
   if (!m.dev_params) {
     e = cudaMalloc(&m.dev_params, m.params.size() * sizeof(float));
     if (e == cudaSuccess)
       e = cudaMemcpy(m.dev_params, m.params.data(),
                      m.params.size() * sizeof(float), cudaMemcpyHostToDevice);
+    void *h = nullptr, *d = nullptr;
     if (e == cudaSuccess)
-      e = cudaMalloc(&m.dev_x, TEMPI_MLP_IN * sizeof(float));
+      e = cudaHostAlloc(&h, io_floats * sizeof(float), cudaHostAllocMapped);
     if (e == cudaSuccess)
-      e = cudaMalloc(&m.dev_out, size_t(m.members) * TEMPI_MLP_OUT * sizeof(float));
-    if (e != cudaSuccess)
+      e = cudaHostGetDevicePointer(&d, h, 0);
+    if (e != cudaSuccess) {
+      if (h)
+        cudaFreeHost(h);
+      cudaFree(m.dev_params);
+      m.dev_params = nullptr;
       return cuda_error(e, "cost model upload");
+    }
+    m.host_io = static_cast<float *>(h);
+    m.dev_io = static_cast<float *>(d);
   }
   cudaStream_t s = pack_stream();
-  float out[64 * TEMPI_MLP_OUT];
-  e = cudaMemcpyAsync(m.dev_x, f, TEMPI_MLP_IN * sizeof(float),
-                      cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess)
-    return cuda_error(e, "cost model input");
-  int err = tempi_mlp_predict(m.dev_params, m.members, m.dev_x, 1, m.dev_out, s);
+  std::memcpy(m.host_io, f, TEMPI_MLP_IN * sizeof(float));
+  std::atomic_thread_fence(std::memory_order_seq_cst); // before the launch
+  int err = tempi_mlp_predict(m.dev_params, m.members, m.dev_io, 1,
+                              m.dev_io + TEMPI_MLP_IN, s);
   if (err)
     return err;
-  e = cudaMemcpyAsync(out, m.dev_out,
-                      size_t(m.members) * TEMPI_MLP_OUT * sizeof(float),
-                      cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess)
-    e = cudaStreamSynchronize(s);
+  e = cudaStreamSynchronize(s);
   if (e != cudaSuccess)
     return cuda_error(e, "cost model output");
+  const float *out = m.host_io + TEMPI_MLP_IN;
   for (int j = 0; j < TEMPI_MLP_OUT; ++j) {
     double s1 = 0, s2 = 0;
     for (int k = 0; k < m.members; ++k) {
@@ -349,6 +366,37 @@ tempi_config choose_config(const tempi_desc &d, int64_t incount) {
   return tempi_config{}; // the fixed rules in launch_geometry
 }
 
+// The layout cache's key: the descriptor's fields in use, the object count,
+// the buffer kinds, what is chosen ('p' pack, 'u' unpack, 'm' method) and
+// the policy.
+std::string layout_key(const tempi_desc &d, int64_t n, bool a, bool b,
+                       char what) {
+  int64_t v[5 + 2 * TEMPI_MAX_DIMS];
+  int k = 0;
+  v[k++] = d.start;
+  v[k++] = d.extent;
+  v[k++] = d.block;
+  v[k++] = d.ndims;
+  v[k++] = n;
+  for (int i = 0; i < d.ndims && i < TEMPI_MAX_DIMS; ++i) {
+    v[k++] = d.counts[i];
+    v[k++] = d.strides[i];
+  }
+  std::string key(reinterpret_cast<const char *>(v), size_t(k) * sizeof(int64_t));
+  key.push_back(char(a));
+  key.push_back(char(b));
+  key.push_back(what);
+  key.push_back(char(env().dispatch));
+  return key;
+}
+
+// under g_mu
+void remember_layout(const std::string &key, int choice) {
+  if (g_layouts.size() >= kMaxLayouts)
+    g_layouts.clear();
+  g_layouts[key] = choice;
+}
+
 tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
                            bool dst_host, bool unpack) {
   const Dispatch mode = env().dispatch;
@@ -356,12 +404,22 @@ tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
     return tempi_config{};
   const uint64_t key = config_key(incount, src_host, dst_host, unpack);
   const int lo = unpack ? kUnpackOut : kPackOut;
+  const std::string lkey =
+      layout_key(r.desc, incount, src_host, dst_host, unpack ? 'u' : 'p');
+  const std::string lkey2 =
+      layout_key(r.desc, incount, src_host, dst_host, unpack ? 'p' : 'u');
   {
     std::lock_guard<std::mutex> l(g_mu);
     auto it = r.configs.find(key);
     if (it != r.configs.end()) {
       counters().dispatch_hit++;
       return it->second < 0 ? tempi_config{} : kCandidates[it->second];
+    }
+    auto lt = g_layouts.find(lkey); // another handle of the same layout
+    if (lt != g_layouts.end()) {
+      counters().dispatch_hit++;
+      r.configs[key] = lt->second;
+      return lt->second < 0 ? tempi_config{} : kCandidates[lt->second];
     }
   }
   counters().dispatch_miss++;
@@ -385,6 +443,7 @@ tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
         std::lock_guard<std::mutex> l(g_mu);
         r.configs.emplace(config_key(incount, src_host, dst_host, !unpack),
                           other);
+        remember_layout(lkey2, other);
       }
     }
   }
@@ -406,10 +465,12 @@ tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
           other = j;
       std::lock_guard<std::mutex> l(g_mu);
       r.configs[config_key(incount, src_host, dst_host, !unpack)] = other;
+      remember_layout(lkey2, other);
     }
   }
   std::lock_guard<std::mutex> l(g_mu);
   r.configs[key] = choice;
+  remember_layout(lkey, choice);
   return choice < 0 ? tempi_config{} : kCandidates[choice];
 }
 
@@ -425,12 +486,19 @@ Method choose_method(TypeRecord &r, int count) {
     break;
   }
   const int64_t bytes = int64_t(count) * r.desc.size;
+  const std::string lkey = layout_key(r.desc, count, false, false, 'm');
   {
     std::lock_guard<std::mutex> l(g_mu);
     auto it = r.methods.find(bytes);
     if (it != r.methods.end()) {
       counters().dispatch_hit++;
       return it->second;
+    }
+    auto lt = g_layouts.find(lkey);
+    if (lt != g_layouts.end()) {
+      counters().dispatch_hit++;
+      r.methods[bytes] = Method(lt->second);
+      return Method(lt->second);
     }
   }
   counters().dispatch_miss++;
@@ -453,6 +521,7 @@ Method choose_method(TypeRecord &r, int count) {
   }
   std::lock_guard<std::mutex> l(g_mu);
   r.methods[bytes] = m;
+  remember_layout(lkey, int(m));
   return m;
 }
 
