@@ -29,6 +29,8 @@ Also reported on the same GPU in the same run:
              and of the fixed rules against exhaustive measurement
   vector_1024x64  the 1024 x 64 B vector (stride 512) through the interposer
              on host buffers (the library's host pack) and on device buffers
+  type_commit  MPI_Type_commit cost: one shape committed repeatedly, and
+             fresh shapes (one cost-model inference each)
   cpu_baseline  the oracle's C type-map walker (a port of what the underlying
              MPI's host MPI_Pack does) on one host core, on a bounded sample
 
@@ -777,6 +779,33 @@ def vector_1024x64_bench(torch, mpi, reps=200):
                 timing="host wall clock per MPI_Pack+MPI_Unpack pair, 200 pairs")
 
 
+def type_commit_bench(mpi, reps=200):
+    """MPI_Type_commit + MPI_Type_free through the interposer, as the
+    reference's bin/bench_type_commit.cpp times them: a 3-D subarray committed
+    again and again (the learned dispatch's choice is reused), and `reps`
+    subarrays of distinct shapes (each one inference of the cost model)."""
+    import time as _t
+
+    def timed(make):
+        t = make()
+        a = _t.perf_counter()
+        assert mpi.Type_commit(t) == 0
+        b = _t.perf_counter()
+        mpi.Type_free(t)
+        return b - a
+
+    same = [timed(lambda: mpi.Type_create_subarray([256, 256, 256], [256, 256, 16], [0, 0, 3],
+                                                  mpi.ORDER_C, mpi.FLOAT))
+            for _ in range(reps)]
+    fresh = [timed(lambda i=i: mpi.Type_create_subarray([256, 256, 256],
+                                                       [256, 1 + i % 255, 3 + i // 255],
+                                                       [0, 0, 0], mpi.ORDER_C, mpi.FLOAT))
+             for i in range(reps)]
+    return {"repeated_shape_commit_us": round(1e6 * float(np.median(same)), 2),
+            "new_shape_commit_us": round(1e6 * float(np.median(fresh)), 2),
+            "reps": reps, "timing": "host wall clock, median"}
+
+
 def reduce_max(value, dist, device=None):
     """Max over ranks of a per-rank time (replicas: one process per GPU)."""
     if dist is None:
@@ -863,6 +892,7 @@ def run_ours(args):
     e2e = dict(e2e_zc, staged=e2e_staged)
     send_res = sendrecv_bench(torch, mpi) if solo and not args.no_sendrecv else None
     c1_res = vector_1024x64_bench(torch, mpi) if solo else None
+    commit_res = type_commit_bench(mpi) if solo else None
     disp_res = dispatch_sample(torch) if solo and not args.no_sendrecv else None
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
@@ -883,6 +913,7 @@ def run_ours(args):
         "e2e": e2e,
         "halo": halo_res,
         "vector_1024x64": c1_res,
+        "type_commit": commit_res,
         "sendrecv": send_res,
         "dispatch": disp_res,
         "sweep": [{"p": r["label"], "k": r["kernel"], "pack_gbs": round(r["pack_gbs"], 1),
