@@ -100,3 +100,33 @@ def test_learned_beats_fixed_rules_on_fresh_layouts(model):
     print(f"total-time regret: learned {learned:.3f}, fixed rules {fixed:.3f}")
     assert learned < fixed
     assert learned < 0.10
+
+
+def test_layout_cache_serves_a_new_handle_of_a_known_shape(model):
+    """A second handle of a layout committed before takes the choices made
+    for the first (no inference, no measurement): MPI_Type_commit of the
+    same shape again counts only dispatch hits, and the pack through the new
+    handle is still exact."""
+    import torch
+
+    def make():
+        return mpi.Type_create_subarray([64, 64, 64], [64, 48, 24], [0, 5, 7],
+                                        mpi.ORDER_C, mpi.FLOAT)
+
+    t1 = make()
+    assert mpi.Type_commit(t1) == 0
+    miss0, hit0 = _lib.counter("dispatch_miss"), _lib.counter("dispatch_hit")
+    t2 = make()
+    assert mpi.Type_commit(t2) == 0
+    assert _lib.counter("dispatch_miss") == miss0
+    assert _lib.counter("dispatch_hit") > hit0
+    o = T.subarray([64, 64, 64], [64, 48, 24], [0, 5, 7], T.ORDER_C, T.FLOAT)
+    src_np = H.splitmix_bytes(o.extent + 64, 12)
+    src = torch.from_numpy(src_np).cuda()
+    out = torch.zeros(o.size, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    e, pos = mpi.Pack(src.data_ptr(), 1, t2, out.data_ptr(), out.numel())
+    assert e == 0 and pos == o.size
+    assert out.cpu().numpy().tobytes() == T.pack(o, src_np, 1).tobytes()
+    mpi.Type_free(t1)
+    mpi.Type_free(t2)
