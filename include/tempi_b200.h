@@ -169,11 +169,16 @@ int tempi_batch_create_copy(const tempi_copy_region *regions, int32_t n,
    an application whose memory pool already owns the GPU's memory -- the
    region table is kept in a fixed array inside the library instead of
    memory from cudaMalloc.  At most 1024 regions per call (larger n returns
-   TEMPI_ERR_ARG).  Every GPU that loads the library holds that 168 KiB
-   array until exit.  The first call on a device, with that device current,
-   looks up the array's device address, so make it before any stream
-   capture.  All calls share the array: calls whose launches can overlap on
-   the GPU race on it. */
+   TEMPI_ERR_ARG, and so does any invalid region, before anything is
+   launched).  Every GPU that loads the library holds that 168 KiB array
+   until exit.  The table reaches the array through the parameters of small
+   fill kernels (one per 128 regions) launched on `stream` ahead of the
+   batch kernel, so the call copies nothing from host memory and never
+   waits for earlier work on the stream.  The first call on a device, with
+   that device current, looks up the array's device address, so make it
+   before any stream capture; that address is not looked up again after a
+   cudaDeviceReset.  All calls share the array: calls whose launches can
+   overlap on the GPU race on it. */
 int tempi_batch_run_static(const tempi_region *regions, int32_t n,
                            int32_t unpack, void *stream);
 

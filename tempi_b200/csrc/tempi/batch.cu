@@ -531,16 +531,46 @@ extern "C" int tempi_batch_replay(tempi_batch *b, void *stream) {
 // each device, with that device current, asks the runtime for the array's
 // device address once (cudaGetSymbolAddress) and every call passes that
 // address to the kernel.  Because of that set-up, the first call on a
-// device should come before any stream capture.  All calls share the one
+// device should come before any stream capture.  The cached address is not
+// refreshed if the application resets the device (cudaDeviceReset).
+//
+// The table reaches the array without a host-to-device copy: the host
+// builds it in pieces of up to kFillPiece entries and passes each piece BY
+// VALUE as the parameter of a small kernel (k_static_fill) that writes it
+// into the array, on the caller's stream ahead of the batch kernel.  Kernel
+// parameters are copied when the launch is issued, so the host's piece can
+// be reused at once, and the host never waits for earlier work on the
+// stream (a copy from pageable host memory would).  All calls share the one
 // array and it keeps the last call's table; each call rewrites every entry
 // it uses, so nothing needs clearing, but calls whose launches can overlap
 // on the GPU (different streams, no ordering) race on the table.
 constexpr int kStaticBatchRegions = 1024;
 constexpr int kMaxDevices = 64;
+constexpr int kFillPiece = 128; // 21.5 KB of parameters (the limit is 32,764 B)
 
 static_assert(sizeof(BatchRegion) == 168 && sizeof(BatchRegion) % 4 == 0,
               "table entry size is documented");
 static __device__ __align__(256) BatchRegion g_static_regions[kStaticBatchRegions];
+
+template <int P> struct StaticPiece {
+  BatchRegion r[P];
+};
+static_assert(sizeof(StaticPiece<kFillPiece>) + 8 <= 32764,
+              "a piece fits the kernel parameter space");
+
+// entries [first, first + count) of the array from the piece, a 32-bit
+// word per thread; the host guarantees first + count <= kStaticBatchRegions
+// and count <= P
+template <int P>
+__global__ void __launch_bounds__(256)
+    k_static_fill(const __grid_constant__ StaticPiece<P> piece, int first,
+                  int count) {
+  constexpr int kWords = sizeof(BatchRegion) / 4;
+  const uint32_t *from = reinterpret_cast<const uint32_t *>(piece.r);
+  uint32_t *to = reinterpret_cast<uint32_t *>(g_static_regions + first);
+  for (int w = threadIdx.x; w < count * kWords; w += blockDim.x)
+    to[w] = from[w];
+}
 
 static std::mutex g_static_mu;
 static BatchRegion *g_static_ptr[kMaxDevices] = {};
@@ -564,6 +594,23 @@ static int static_table(BatchRegion **out) {
   return TEMPI_OK;
 }
 
+// launch k_static_fill for entries [first, first + count) of `piece`
+static int static_fill(const StaticPiece<kFillPiece> &piece, int first,
+                       int count, cudaStream_t s) {
+  if (count <= 32) { // a small table: a 5.4 KB parameter block
+    StaticPiece<32> small;
+    std::memcpy(small.r, piece.r, size_t(count) * sizeof(BatchRegion));
+    k_static_fill<32><<<1, 256, 0, s>>>(small, first, count);
+  } else {
+    k_static_fill<kFillPiece><<<1, 256, 0, s>>>(piece, first, count);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return cuda_error(e, "static region table fill");
+  counters().kernel_launches++;
+  return TEMPI_OK;
+}
+
 extern "C" int tempi_batch_run_static(const tempi_region *regions, int32_t n,
                                       int32_t unpack, void *stream) {
   if (n < 0 || (n > 0 && !regions))
@@ -577,48 +624,45 @@ extern "C" int tempi_batch_run_static(const tempi_region *regions, int32_t n,
   if (err)
     return err;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // build the table in fixed-size pieces on the stack and copy each piece;
-  // cudaMemcpyAsync from pageable memory returns once the piece is staged,
-  // so the stack buffer can be reused straight away
-  constexpr int kPiece = 32;
-  BatchRegion piece[kPiece];
+  // every region is checked before anything is launched, so a bad region
+  // leaves the array and the stream untouched
+  StaticPiece<kFillPiece> piece;
   int used = 0, filled = 0;
   uint64_t chunks = 0;
-  for (int32_t i = 0; i < n; ++i) {
-    const tempi_region &r = regions[i];
-    BatchRegion &br = piece[filled];
-    br = BatchRegion{};
-    char *strided = (char *)r.origin + r.desc.start;
-    bool empty = false;
-    err = make_geometry(&r.desc, r.incount, uintptr_t(strided),
-                        uintptr_t(r.packed), 0, &br.g, &empty);
-    if (err)
-      return err;
-    if (empty)
-      continue;
-    br.strided = strided;
-    br.packed = (char *)r.packed;
-    br.chunk_begin = uint32_t(chunks);
-    chunks += (br.g.total_words + kChunkWords - 1) / kChunkWords;
-    if (chunks > UINT32_MAX)
-      return set_error(TEMPI_ERR_ARG, "batch too large");
-    if (++filled == kPiece || i == n - 1) {
-      cudaError_t e = cudaMemcpyAsync(table + used, piece,
-                                      filled * sizeof(BatchRegion),
-                                      cudaMemcpyHostToDevice, s);
-      if (e != cudaSuccess)
-        return cuda_error(e, "static region table upload");
+  for (int pass = 0; pass < 2; ++pass) {
+    used = filled = 0;
+    chunks = 0;
+    for (int32_t i = 0; i < n; ++i) {
+      const tempi_region &r = regions[i];
+      BatchRegion &br = piece.r[filled];
+      br = BatchRegion{};
+      char *strided = (char *)r.origin + r.desc.start;
+      bool empty = false;
+      err = make_geometry(&r.desc, r.incount, uintptr_t(strided),
+                          uintptr_t(r.packed), 0, &br.g, &empty);
+      if (err)
+        return err;
+      if (empty)
+        continue;
+      br.strided = strided;
+      br.packed = (char *)r.packed;
+      br.chunk_begin = uint32_t(chunks);
+      chunks += (br.g.total_words + kChunkWords - 1) / kChunkWords;
+      if (chunks > UINT32_MAX)
+        return set_error(TEMPI_ERR_ARG, "batch too large");
+      if (++filled == kFillPiece) {
+        if (pass == 1 && (err = static_fill(piece, used, filled, s)))
+          return err;
+        used += filled;
+        filled = 0;
+      }
+    }
+    if (filled) { // a partial last piece (empty regions are never stored)
+      if (pass == 1 && (err = static_fill(piece, used, filled, s)))
+        return err;
       used += filled;
       filled = 0;
     }
-  }
-  if (filled) { // the last regions were empty ones after a partial piece
-    cudaError_t e = cudaMemcpyAsync(table + used, piece,
-                                    filled * sizeof(BatchRegion),
-                                    cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess)
-      return cuda_error(e, "static region table upload");
-    used += filled;
   }
   if (used == 0)
     return TEMPI_OK;
