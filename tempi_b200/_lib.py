@@ -84,6 +84,18 @@ class Config(ctypes.Structure):
     ]
 
 
+# The cost model's ten kernel configurations, in the order of its outputs
+# (kCandidates in csrc/tempi/dispatch.cpp): word kernel at 256, 512 and 128
+# threads; row kernel; shift kernel at 4, 8, 16, 32 lanes per row; staged
+# kernel at 3 and 8 CTAs per SM.
+CANDIDATE_CONFIGS = (
+    (1, 0, 256, 0, 0, 0), (1, 0, 512, 0, 0, 0), (1, 0, 128, 0, 0, 0),
+    (2, 0, 256, 0, 0, 0),
+    (3, 0, 256, 4, 0, 0), (3, 0, 256, 8, 0, 0), (3, 0, 256, 16, 0, 0), (3, 0, 256, 32, 0, 0),
+    (4, 0, 256, 0, 3, 0), (4, 0, 256, 0, 8, 0),
+)
+
+
 class Region(ctypes.Structure):
     """``tempi_region``."""
 
@@ -183,6 +195,9 @@ _TEMPI_SIGS = {
     "tempi_batch_destroy": (c_int, [c_void_p]),
     "tempi_batch_run_static": (c_int, [P(Region), ctypes.c_int32, ctypes.c_int32, c_void_p]),
     "tempi_batch_create_copy": (c_int, [P(CopyRegion), ctypes.c_int32, P(c_void_p)]),
+    "tempi_batch_tune": (c_int, [c_void_p, c_void_p, ctypes.c_int32]),
+    "tempi_batch_config": (c_int, [c_void_p, P(ctypes.c_int32), P(ctypes.c_int32),
+                                   P(ctypes.c_int32), P(ctypes.c_int32), ctypes.c_int32]),
     "tempi_last_error": (ctypes.c_char_p, []),
     "tempi_kernel_launches": (c_int64, []),
     "tempi_last_kernel": (ctypes.c_char_p, []),

@@ -81,6 +81,20 @@ class Grid:
         return out
 
 
+def mixed_shapes(seed=8, count=8):
+    """(interior, radius) of the mixed halo batch: `count` grids whose
+    interior dimensions are each drawn log-uniform from [32, 512] and whose
+    radius is drawn from 1..3, all from one seed."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        interior = [int(round(np.exp(rng.uniform(np.log(32), np.log(512))))) for _ in range(3)]
+        out.append((interior, int(rng.integers(1, 4))))
+    return out
+
+
 def regions(grids, grid_ptrs, packed_ptrs, unpack=False):
     """tempi_region entries for every region of every grid.  For unpack the
     bytes packed for direction d land in the ghost region of direction -d
@@ -121,6 +135,21 @@ class HaloBatch:
 
     def replay(self, stream):
         _lib.check(_lib.tempi().tempi_batch_replay(self.h, stream), "tempi_batch_replay")
+
+    def tune(self, stream=None, reps=5):
+        """Time the launch shapes and per-class chunk passes (tempi_batch_tune)
+        and keep the fastest; a captured graph must be captured again."""
+        _lib.check(_lib.tempi().tempi_batch_tune(self.h, stream, reps), "tempi_batch_tune")
+
+    def config(self):
+        """(threads per block, blocks per SM, {region class: passes})."""
+        th, cps = ctypes.c_int32(), ctypes.c_int32()
+        cls, ps = (ctypes.c_int32 * 40)(), (ctypes.c_int32 * 40)()
+        n = _lib.tempi().tempi_batch_config(self.h, ctypes.byref(th), ctypes.byref(cps), cls,
+                                            ps, 40)
+        if n < 0:
+            raise RuntimeError(_lib.last_error())
+        return th.value, cps.value, {cls[i]: ps[i] for i in range(n)}
 
     def close(self):
         if self.h:

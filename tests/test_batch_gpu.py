@@ -227,3 +227,97 @@ def test_batch_random_regions(cuda, mpi_init, unpack):
             if n:
                 desc_unpack(d, packed_np[off: off + d.size * n], want[b:], n)
         assert typed.cpu().numpy().tobytes() == want.tobytes()
+
+
+def test_tuned_batch_is_exact_and_remembered(cuda, mpi_init, tmp_path):
+    """tempi_batch_tune times launch shapes and per-class chunk passes on the
+    batch itself and keeps the fastest: the batch's output stays the oracle's
+    (pack and ghost unpack), its choices are reported per region class, and a
+    new batch of the same signature starts with them; capture works again
+    after tuning.  The tuning file goes to a scratch TEMPI_CACHE_DIR."""
+    import os
+
+    import torch
+
+    lib = _lib.tempi()
+    old = os.environ.get("TEMPI_CACHE_DIR")
+    os.environ["TEMPI_CACHE_DIR"] = str(tmp_path)
+    lib.tempi_reload_env()
+    try:
+        g = halo.Grid((40, 33, 17), 2)
+        data_np = H.splitmix_bytes(g.nbytes, 404)
+        data = torch.from_numpy(data_np).cuda()
+        packed = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
+        b = halo.HaloBatch([g], [data.data_ptr()], [packed.data_ptr()])
+        th0, cps0, cls0 = b.config()
+        assert th0 in (128, 256, 512) and set(cls0.values()) <= {1, 2, 4}
+        b.tune(None, 2)
+        th, cps, cls = b.config()
+        assert th in (128, 256, 512) and cps >= 0 and set(cls) == set(cls0)
+        assert set(cls.values()) <= {1, 2, 4}
+        b.launch()
+        torch.cuda.synchronize()
+        want = oracle_pack(g, data_np)
+        assert packed.cpu().numpy().tobytes() == want.tobytes()
+        s = torch.cuda.Stream()
+        packed.zero_()
+        b.capture(s.cuda_stream)
+        b.replay(s.cuda_stream)
+        s.synchronize()
+        assert packed.cpu().numpy().tobytes() == want.tobytes()
+        # a new batch over other buffers with the same regions: same choices
+        data2 = torch.from_numpy(H.splitmix_bytes(g.nbytes, 405)).cuda()
+        packed2 = torch.zeros_like(packed)
+        b2 = halo.HaloBatch([g], [data2.data_ptr()], [packed2.data_ptr()])
+        assert b2.config() == (th, cps, cls)
+        b2.launch()
+        torch.cuda.synchronize()
+        assert packed2.cpu().numpy().tobytes() == oracle_pack(g, data2.cpu().numpy()).tobytes()
+        assert (tmp_path / "tempi_b200_batch_tune.txt").exists()
+        # the tuned unpack into ghost cells
+        ghost = data.clone()
+        ub = halo.HaloBatch([g], [ghost.data_ptr()], [packed.data_ptr()], unpack=True)
+        ub.tune(None, 2)
+        ub.launch()
+        torch.cuda.synchronize()
+        assert ghost.cpu().numpy().tobytes() == oracle_unpack(g, want, data_np).tobytes()
+        b.close()
+        b2.close()
+        ub.close()
+    finally:
+        if old is None:
+            os.environ.pop("TEMPI_CACHE_DIR", None)
+        else:
+            os.environ["TEMPI_CACHE_DIR"] = old
+        lib.tempi_reload_env()
+
+
+def test_tuned_copy_batch_is_exact(cuda, mpi_init, tmp_path):
+    """The fused exchange (a copy batch) tuned the same way still leaves the
+    oracle's grid."""
+    import os
+
+    import torch
+
+    lib = _lib.tempi()
+    old = os.environ.get("TEMPI_CACHE_DIR")
+    os.environ["TEMPI_CACHE_DIR"] = str(tmp_path)
+    lib.tempi_reload_env()
+    try:
+        g = halo.Grid((30, 20, 10), 3)
+        data_np = H.splitmix_bytes(g.nbytes, 77)
+        data = torch.from_numpy(data_np).cuda()
+        x = halo.HaloExchange([g], [data.data_ptr()])
+        x.tune(None, 2)
+        data.copy_(torch.from_numpy(data_np))
+        x.launch()
+        torch.cuda.synchronize()
+        assert data.cpu().numpy().tobytes() == oracle_unpack(g, oracle_pack(g, data_np),
+                                                              data_np).tobytes()
+        x.close()
+    finally:
+        if old is None:
+            os.environ.pop("TEMPI_CACHE_DIR", None)
+        else:
+            os.environ["TEMPI_CACHE_DIR"] = old
+        lib.tempi_reload_env()
