@@ -205,19 +205,22 @@ def cpu_model():
 
 def cpu_baseline(budget_s=12.0):
     """Single-core C walker on the sweep with incount 1 per point, repeated
-    for about `budget_s` seconds."""
+    for about `budget_s` seconds (at least 20 passes); the rate of the median
+    pass."""
     items = _oracle_points(sweep_points(), incount_cap=1)
     bufs = cpu_buffers(items)
     cpu_walk_step(items, bufs, 1)  # warm
     t0 = time.perf_counter()
-    nbytes, reps = 0, 0
-    while time.perf_counter() - t0 < budget_s or reps == 0:
-        nbytes += cpu_walk_step(items, bufs, 1)
-        reps += 1
+    times, nbytes = [], 0
+    while time.perf_counter() - t0 < budget_s or len(times) < 20:
+        a = time.perf_counter()
+        nbytes = cpu_walk_step(items, bufs, 1)
+        times.append(time.perf_counter() - a)
     dt = time.perf_counter() - t0
-    return {"value": round(nbytes / dt / 1e9, 3), "unit": "GB/s", "cores": 1, "kind": "port",
-            "sample": f"{reps} passes over the {len(items)} sweep points at incount 1 "
-                      f"({dt:.1f} s), pack + unpack, oracle/typemap.c single thread",
+    med = statistics.median(times)
+    return {"value": round(nbytes / med / 1e9, 3), "unit": "GB/s", "cores": 1, "kind": "port",
+            "sample": f"median of {len(times)} passes over the {len(items)} sweep points at "
+                      f"incount 1 ({dt:.1f} s), pack + unpack, oracle/typemap.c single thread",
             "cpu": cpu_model()}
 
 
@@ -338,91 +341,307 @@ def time_events(torch, stream, fn, reps, flush=None):
     return sum(ts) / len(ts)
 
 
+def learned_configs(lib, d, n):
+    """The kernel configurations MPI_Pack and MPI_Unpack run for `n` objects
+    of `d` on device buffers (the learned dispatch's picks), as tempi_config
+    structures (None: the fixed rules)."""
+    from tempi_b200 import _lib
+
+    pc, uc, mi = ctypes.c_int(-1), ctypes.c_int(-1), ctypes.c_int(0)
+    _lib.check(lib.tempi_dispatch_choose(ctypes.byref(d), n, 0, 0, 0, ctypes.byref(pc),
+                                         ctypes.byref(uc), ctypes.byref(mi), None, None))
+    out = []
+    for k in (pc.value, uc.value):
+        out.append(_lib.Config(*_lib.CANDIDATE_CONFIGS[k]) if k >= 0 else None)
+    return out
+
+
+def line_traffic(sizes, subs, starts, incount, unpack, elem=4, line=128, sector=32):
+    """DRAM bytes a pack (or unpack) of `incount` C-order subarray objects
+    cannot avoid, a lower bound: a pack reads every 128-B line its rows
+    touch (ncu shows L2 fetching whole lines for rows scattered this far
+    apart) and writes the packed bytes; an unpack reads the packed bytes and
+    writes every 32-B sector its rows touch (the reads that merge partial
+    sectors are not counted).  Dimensions whose subarray spans the full
+    extent merge into longer runs.  Every run starts at the same offset
+    modulo 128 (the sweep's row pitches and extents are multiples of 128 B,
+    and buffers are 128-B aligned)."""
+    nd = len(sizes)
+    k = nd - 1
+    run = subs[k] * elem
+    off = (starts[k] * elem) % line if subs[k] != sizes[k] else 0
+    while k > 0 and subs[k] == sizes[k]:
+        run *= subs[k - 1]
+        k -= 1
+    runs = incount * int(np.prod(subs[:k])) if k > 0 else incount
+    packed = runs * run
+    if not unpack:
+        return runs * line * (-(-(off + run) // line)) + packed
+    so = off % sector
+    return packed + runs * sector * (-(-(so + run) // sector))
+
+
+def empty_kernel_events(torch, sw, stream, reps=20):
+    """Median CUDA-event time (ms) of one empty kernel launched the way the
+    per-point kernels are timed (L2 flushed first): the fixed cost of a
+    timed launch on this GPU."""
+    ts = []
+    for _ in range(reps):
+        sw.flush_l2(stream)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        driver().tempi_bench_empty(stream.cuda_stream)
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
 def kernel_table(torch, sw, stream, lib, reps=5):
-    """Per-point pack and unpack kernel times through tempi_pack/unpack."""
+    """Per point: the pack and the unpack kernel that MPI_Pack / MPI_Unpack
+    run (the learned dispatch's picks), each launched alone through
+    tempi_pack/tempi_unpack with the L2 flushed first, CUDA events around
+    the launch (`call`: the event pair and the launch's own fixed cost
+    included); the line-traffic bound of the layout; and, where the committed
+    launch list (profiles/kernel_times.txt) has the point, ncu's in-kernel
+    duration."""
     from tempi_b200 import _lib, mpi
 
     rows = []
     s = stream.cuda_stream
+    ktimes = kernel_times_from_profiles()
     for p in sw.pts:
         err, d = mpi.describe(p["t"])
         assert err == 0
         n = p["incount"]
+        cp, cu = learned_configs(lib, d, n)
         pk = lambda: _lib.check(lib.tempi_pack(ctypes.byref(d), p["src"].data_ptr(), n,
-                                               sw.packed.data_ptr(), None, s))
+                                               sw.packed.data_ptr(),
+                                               ctypes.byref(cp) if cp else None, s))
         up = lambda: _lib.check(lib.tempi_unpack(ctypes.byref(d), sw.packed.data_ptr(), n,
-                                                 p["dst"].data_ptr(), None, s))
+                                                 p["dst"].data_ptr(),
+                                                 ctypes.byref(cu) if cu else None, s))
         pk()
         kname = lib.tempi_last_kernel().decode()
+        up()
+        uname = lib.tempi_last_kernel().decode()
         t_pack = time_events(torch, stream, pk, reps, lambda: sw.flush_l2(stream))
         t_unpack = time_events(torch, stream, up, reps, lambda: sw.flush_l2(stream))
         alg = 2 * p["size"] * n
-        rows.append(dict(label=p["label"], packed_bytes=p["size"] * n, kernel=kname,
-                         pack_ms=t_pack, unpack_ms=t_unpack,
-                         pack_gbs=alg / t_pack / 1e6, unpack_gbs=alg / t_unpack / 1e6))
+        tr = [line_traffic(p["sizes"], p["subs"], p["starts"], n, u) for u in (0, 1)]
+        row = dict(label=p["label"], packed_bytes=p["size"] * n, kernel=kname, ukernel=uname,
+                   pack_ms=t_pack, unpack_ms=t_unpack,
+                   pack_gbs=alg / t_pack / 1e6, unpack_gbs=alg / t_unpack / 1e6,
+                   line_bound=[alg / t for t in tr], traffic=tr)  # fractions of the peak
+        for direction in ("pack", "unpack"):
+            us = ktimes.get((p["label"], direction))
+            if us:
+                row[direction + "_kernel_us"] = us
+        rows.append(row)
     return rows
 
 
-def halo_bench(torch, stream, reps=20):
+def point_bound(empty_us, gather_us, traffic, peak):
+    """Least in-kernel time (us) of a launch that moves `traffic` DRAM
+    bytes: a launch's fixed cost (an empty kernel) plus the traffic at the
+    copy peak, and never less than a kernel that reads one scattered line
+    per thread and stores it (one DRAM round trip)."""
+    return max(empty_us + traffic / peak / 1e3, gather_us)
+
+
+def sweep_row(r, peak):
+    """The bench line's entry for one sweep point."""
+    out = {"p": r["label"], "k": r["kernel"], "ku": r["ukernel"],
+           "pack_gbs": round(r["pack_gbs"], 1), "unpack_gbs": round(r["unpack_gbs"], 1),
+           "line_bound": [round(x, 3) for x in r["line_bound"]]}
+    empty, gather = KERNEL_FLOORS_US
+    kg, ob = [], []
+    for u, direction in enumerate(("pack", "unpack")):
+        us = r.get(direction + "_kernel_us")
+        if us:
+            kg.append(round(2 * r["packed_bytes"] / us / 1e3, 1))
+            if empty is not None and gather is not None:
+                ob.append(round(point_bound(empty, gather, r["traffic"][u], peak) / us, 3))
+    if len(kg) == 2:
+        out["kernel_gbs"] = kg
+        out["kernel_frac"] = [round(x / peak, 3) for x in kg]
+    if len(ob) == 2:
+        out["of_bound"] = ob
+    return out
+
+
+# in-kernel times of the empty kernel and the one-load gather in the
+# committed launch list (ncu)
+KERNEL_FLOORS_US = [None, None]
+
+
+def dominant_back_to_back(torch, sw, stream, lib, label, k=10, reps=5):
+    """Median over `reps` of (time of `k` back-to-back launches of the
+    point's pack kernel between one event pair) / k, in ms."""
+    from tempi_b200 import _lib, mpi
+
+    p = next(q for q in sw.pts if q["label"] == label)
+    err, d = mpi.describe(p["t"])
+    assert err == 0
+    n = p["incount"]
+    cp, _ = learned_configs(lib, d, n)
+    s = stream.cuda_stream
+
+    def pk():
+        _lib.check(lib.tempi_pack(ctypes.byref(d), p["src"].data_ptr(), n, sw.packed.data_ptr(),
+                                  ctypes.byref(cp) if cp else None, s))
+
+    ts = []
+    for _ in range(reps):
+        sw.flush_l2(stream)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(k):
+            pk()
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b) / k)
+    return statistics.median(ts)
+
+
+def kernel_times_from_profiles():
+    """(point, direction) -> ncu in-kernel microseconds of the kernel the
+    interposer runs, from the committed launch-list summary."""
+    path = os.path.join(ROOT, "profiles", "kernel_times.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            f = line.split()
+            if line.startswith("#") and "empty kernel" in line:
+                KERNEL_FLOORS_US[0] = float(line.split("empty kernel")[1].split()[0])
+                if "gather" in line:
+                    KERNEL_FLOORS_US[1] = float(line.split("gather")[1].split()[0])
+            elif len(f) >= 3 and not line.startswith("#"):
+                out[(f[0], f[1])] = float(f[2])
+    return out
+
+
+def halo_bench(torch, sw, stream, reps=20):
+    """The 256^3-double radius-2 halo (26 regions) and the mixed batch of 8
+    grids, seeded data: plain per-region MPI_Pack / MPI_Unpack calls against
+    one batched launch and one CUDA-graph replay, the L2 flushed before each
+    timed pass.  `bit_exact`: the batched and graph outputs equal the plain
+    path's, byte for byte (compared on the device)."""
     from tempi_b200 import halo
 
-    g = halo.Grid((256, 256, 256), 2)
-    data = torch.randint(0, 256, (g.nbytes,), dtype=torch.uint8, device="cuda")
-    packed = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
-    torch.cuda.synchronize()
-    plain_ops = []
-    pos = 0
-    for d in halo.directions():
-        plain_ops.append(BenchOp(0, g.send[d], data.data_ptr(), packed.data_ptr(), 1, pos,
-                                 g.packed_bytes, 0))
-        pos += g.region_bytes[d]
-    run_ops(plain_ops, 3)
-    t_plain = sum(run_ops(plain_ops, reps)) / reps
-    b = halo.HaloBatch([g], [data.data_ptr()], [packed.data_ptr()])
+    flush = lambda: sw.flush_l2(stream)
     s = stream.cuda_stream
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(256)
+    g = halo.Grid((256, 256, 256), 2)
+    data = torch.randint(0, 256, (g.nbytes,), dtype=torch.uint8, device="cuda", generator=gen)
+    p_plain = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
+    p_batch, p_graph = torch.zeros_like(p_plain), torch.zeros_like(p_plain)
+    torch.cuda.synchronize()
+
+    def plain_ops(grid, dptr, pptr, unpack=False):
+        ops, pos = [], 0
+        for d in halo.directions():
+            t = grid.recv[tuple(-x for x in d)] if unpack else grid.send[d]
+            ops.append(BenchOp(int(unpack), t, dptr, pptr, 1, pos, grid.packed_bytes, 0))
+            pos += grid.region_bytes[d]
+        return ops
+
+    ops = plain_ops(g, data.data_ptr(), p_plain.data_ptr())
+    run_ops(ops, 3)
+    t_plain = statistics.median(run_ops(ops, reps, sw.flush))
+    b = halo.HaloBatch([g], [data.data_ptr()], [p_batch.data_ptr()])
     for _ in range(3):
         b.launch(s)
-    t_batch = time_events(torch, stream, lambda: b.launch(s), reps)
-    b.capture(s)
+    t_batch = time_events(torch, stream, lambda: b.launch(s), reps, flush)
+    bg = halo.HaloBatch([g], [data.data_ptr()], [p_graph.data_ptr()])
+    bg.capture(s)
     for _ in range(3):
-        b.replay(s)
-    t_graph = time_events(torch, stream, lambda: b.replay(s), reps)
+        bg.replay(s)
+    t_graph_default = time_events(torch, stream, lambda: bg.replay(s), reps, flush)
+    cfg_default = bg.config()
+    # the autotuner on this batch (its choices then hold for every batch of
+    # the same regions, the unpack's below included once tuned)
+    bg.tune(s, 5)
+    bg.capture(s)
+    for _ in range(3):
+        bg.replay(s)
+    t_graph = time_events(torch, stream, lambda: bg.replay(s), reps, flush)
+    cfg_tuned = bg.config()
+    torch.cuda.synchronize()
+    pack_exact = bool(torch.equal(p_plain, p_batch) and torch.equal(p_plain, p_graph))
     b.close()
-    # mixed batch of 8 grids: interiors log-uniform in [32, 512], radius 1..3
-    rng = np.random.default_rng(8)
-    grids, datas, packs = [], [], []
-    for _ in range(8):
-        interior = [int(round(np.exp(rng.uniform(np.log(32), np.log(512))))) for _ in range(3)]
-        gg = halo.Grid(interior, int(rng.integers(1, 4)))
-        grids.append(gg)
-        datas.append(torch.empty(gg.nbytes, dtype=torch.uint8, device="cuda"))
-        packs.append(torch.empty(gg.packed_bytes, dtype=torch.uint8, device="cuda"))
-    mb = halo.HaloBatch(grids, [d.data_ptr() for d in datas], [p.data_ptr() for p in packs])
+    bg.close()
+
+    # unpack into the ghost cells: the packed bytes land in the ghost region
+    # opposite their direction, three copies of the grid, one per method
+    grids = [data.clone() for _ in range(3)]
+    uops = plain_ops(g, grids[0].data_ptr(), p_plain.data_ptr(), unpack=True)
+    run_ops(uops, 3)
+    t_uplain = statistics.median(run_ops(uops, reps, sw.flush))
+    ub = halo.HaloBatch([g], [grids[1].data_ptr()], [p_plain.data_ptr()], unpack=True)
+    for _ in range(3):
+        ub.launch(s)
+    t_ubatch = time_events(torch, stream, lambda: ub.launch(s), reps, flush)
+    ug = halo.HaloBatch([g], [grids[2].data_ptr()], [p_plain.data_ptr()], unpack=True)
+    ug.tune(s, 5)
+    ug.capture(s)
+    for _ in range(3):
+        ug.replay(s)
+    t_ugraph = time_events(torch, stream, lambda: ug.replay(s), reps, flush)
+    torch.cuda.synchronize()
+    unpack_exact = bool(torch.equal(grids[0], grids[1]) and torch.equal(grids[0], grids[2])
+                        and not torch.equal(grids[0], data))
+    ub.close()
+    ug.close()
+    del grids
+
+    # mixed batch of 8 grids
+    grids_m = [halo.Grid(interior, r) for interior, r in halo.mixed_shapes()]
+    datas = [torch.randint(0, 256, (gg.nbytes,), dtype=torch.uint8, device="cuda", generator=gen)
+             for gg in grids_m]
+    pk_plain = [torch.zeros(gg.packed_bytes, dtype=torch.uint8, device="cuda") for gg in grids_m]
+    pk_graph = [torch.zeros_like(x) for x in pk_plain]
+    mb = halo.HaloBatch(grids_m, [d.data_ptr() for d in datas], [p.data_ptr() for p in pk_graph])
+    mb.tune(s, 5)
     mb.capture(s)
     for _ in range(3):
         mb.replay(s)
-    t_mixed = time_events(torch, stream, lambda: mb.replay(s), reps)
-
+    t_mixed = time_events(torch, stream, lambda: mb.replay(s), reps, flush)
     mixed_ops = []
-    for gg, dd, pp in zip(grids, datas, packs):
-        pos = 0
-        for d in halo.directions():
-            mixed_ops.append(BenchOp(0, gg.send[d], dd.data_ptr(), pp.data_ptr(), 1, pos,
-                                     gg.packed_bytes, 0))
-            pos += gg.region_bytes[d]
+    for gg, dd, pp in zip(grids_m, datas, pk_plain):
+        mixed_ops += plain_ops(gg, dd.data_ptr(), pp.data_ptr())
     run_ops(mixed_ops, 2)
-    t_mixed_plain = sum(run_ops(mixed_ops, 5)) / 5
+    t_mixed_plain = statistics.median(run_ops(mixed_ops, 5, sw.flush))
+    torch.cuda.synchronize()
+    mixed_exact = all(torch.equal(x, y) for x, y in zip(pk_plain, pk_graph))
     mb.close()
-    del datas, packs
+    del datas, pk_plain, pk_graph
+    mixed_bytes = int(sum(gg.packed_bytes for gg in grids_m))
     return {
-        "grid": "256^3 doubles, radius 2, 26 regions, 6390272 B packed",
+        "grid": "256^3 doubles, radius 2, 26 regions, 6390272 B packed, seeded data",
+        "timing": "median of %d passes, L2 flushed before each, CUDA events" % reps,
         "plain_us": round(1e3 * t_plain, 2), "batched_us": round(1e3 * t_batch, 2),
         "graph_us": round(1e3 * t_graph, 2),
+        "graph_untuned_us": round(1e3 * t_graph_default, 2),
+        "tuned": {"threads": cfg_tuned[0], "ctas_per_sm": cfg_tuned[1],
+                  "passes_per_class": {str(k): v for k, v in cfg_tuned[2].items()}},
+        "untuned": {"threads": cfg_default[0], "ctas_per_sm": cfg_default[1],
+                    "passes_per_class": {str(k): v for k, v in cfg_default[2].items()}},
+        "class": "8 * log2(vector width) + min(7, log2(words per row))",
         "speedup_graph_vs_plain": round(t_plain / t_graph, 2),
         "graph_gbs": round(2 * g.packed_bytes / t_graph / 1e6, 1),
-        "mixed8_regions": 208, "mixed8_bytes": int(sum(gg.packed_bytes for gg in grids)),
+        "unpack_plain_us": round(1e3 * t_uplain, 2), "unpack_batched_us": round(1e3 * t_ubatch, 2),
+        "unpack_graph_us": round(1e3 * t_ugraph, 2),
+        "unpack_speedup_graph_vs_plain": round(t_uplain / t_ugraph, 2),
+        "bit_exact": pack_exact and unpack_exact and mixed_exact,
+        "bit_exact_parts": {"pack": pack_exact, "unpack": unpack_exact, "mixed8": mixed_exact},
+        "mixed8_regions": 26 * len(grids_m), "mixed8_bytes": mixed_bytes,
         "mixed8_graph_us": round(1e3 * t_mixed, 2),
         "mixed8_plain_us": round(1e3 * t_mixed_plain, 2),
+        "mixed8_speedup_graph_vs_plain": round(t_mixed_plain / t_mixed, 2),
     }
 
 
@@ -458,6 +677,11 @@ def halo_exchange_bench(torch, stream, reps=20):
     n = len(sg.sendtypes)
     base = torch.randint(0, 256, (g.nbytes,), dtype=torch.uint8, device="cuda")
     grids = [base.clone() for _ in range(3)]
+    # tune the fused exchange first: the interposed MPI_Neighbor_alltoallw
+    # below takes the same choices (same copy pairs, same signature)
+    xt = halo.HaloExchange([g], [grids[2].data_ptr()])
+    xt.tune(stream.cuda_stream, 5)
+    xt.close()
     sendbuf = torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
     recvbuf = torch.zeros_like(sendbuf)
     ints = lambda v: (ctypes.c_int * n)(*v)
@@ -502,6 +726,9 @@ def driver():
         _lib.tempi()
         _driver = ctypes.CDLL(os.path.join(ROOT, "tempi_b200", "csrc", "libtempi_bench.so"))
         _driver.tempi_bench_flush.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        _driver.tempi_bench_empty.argtypes = [ctypes.c_void_p]
+        _driver.tempi_bench_gather.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int,
+                                               ctypes.c_void_p, ctypes.c_void_p]
         sz = ctypes.c_size_t
         _driver.tempi_bench_copy2d.argtypes = [ctypes.c_void_p, sz, ctypes.c_void_p, sz, sz, sz,
                                                ctypes.c_int, ctypes.c_void_p]
@@ -599,6 +826,17 @@ def e2e_zero_copy(torch, sw, steps, warmup):
     dma0 = _lib.counter("host_link_copies")
     run_ops(ops, warmup)
     ms = sum(run_ops(ops, steps)) / steps
+    # per point: its MPI_Pack + MPI_Unpack pair alone, against the link: the
+    # packed bytes cross it once each way per call (typed rows in and packed
+    # bytes out, then back), both directions at once
+    link = host_link_both_ways(torch)
+    points = []
+    for i, p in enumerate(sw.pts):
+        n = p["size"] * p["incount"]
+        t = statistics.median(run_ops(ops[2 * i: 2 * i + 2], max(3, steps // 5)))
+        bound_ms = 2 * n / (link * 1e6)
+        points.append({"p": p["label"], "ms": round(t, 4), "gbs": round(4 * n / t / 1e6, 2),
+                       "link_bound_ms": round(bound_ms, 4), "of_link_bound": round(bound_ms / t, 3)})
     # every call ran a pack or unpack kernel, or (a contiguous run between the
     # two host buffers) the copy-engine pipeline; the first call per buffer
     # kind also runs the cost model's inference kernel
@@ -609,6 +847,8 @@ def e2e_zero_copy(torch, sw, steps, warmup):
             "h2d_bytes_per_step": int(2 * nbytes), "d2h_bytes_per_step": int(2 * nbytes),
             "ms_per_step": round(ms, 3),
             "kernel_calls_per_step": round((kernels) / (steps + warmup), 1),
+            "link_gbs_each_way": round(link, 1),
+            "points": points,
             "copy_engine_calls_per_step": round(dma / (steps + warmup), 1),
             "how": "MPI_Pack/MPI_Unpack on pinned host buffers: strided objects by kernels "
                    "that read and write host memory directly; objects of 8 MiB or more that "
@@ -617,9 +857,46 @@ def e2e_zero_copy(torch, sw, steps, warmup):
                    "bytes)"}
 
 
-def sendrecv_bench(torch, mpi, reps=2):
-    """Self-sends (MPI_Isend + MPI_Irecv + MPI_Wait x2) of strided
-    device objects by each method, and the method each policy picks."""
+def host_link_both_ways(torch, nbytes=256 << 20, reps=5):
+    """GB/s per direction of the copy engines moving `nbytes` host->device
+    and device->host at the same time (pinned host memory): the link's
+    rate when both directions are busy, as they are in a pack or unpack
+    between two host buffers."""
+    ha = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    hb = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    da = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    db = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    ts = []
+    for _ in range(reps + 1):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(s1)
+        s2.wait_event(a)
+        with torch.cuda.stream(s1):
+            da.copy_(ha, non_blocking=True)
+        with torch.cuda.stream(s2):
+            hb.copy_(db, non_blocking=True)
+        c = torch.cuda.Event()
+        c.record(s2)
+        s1.wait_event(c)
+        b.record(s1)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    del ha, hb, da, db
+    return nbytes / statistics.median(ts[1:]) / 1e6
+
+
+def sendrecv_bench(torch, mpi, reps=20):
+    """Self-sends (MPI_Isend + MPI_Irecv + MPI_Wait x2) of strided device
+    objects by each method, and what each policy picks.  Every repetition
+    times one round trip per policy, the policies in an order rotated by one
+    each repetition (so no policy always runs first or last), each on a
+    freshly committed type after one untimed round trip; medians per policy.
+    For the ONE_SHOT method, the rate of its pack kernel writing the packed
+    bytes into mapped pinned host memory, against a kernel's contiguous
+    write rate into pinned host memory measured in the same run."""
     import time as _t
 
     from tempi_b200 import _lib
@@ -637,6 +914,9 @@ def sendrecv_bench(torch, mpi, reps=2):
     ]
     knobs = {"DEVICE": "TEMPI_DATATYPE_DEVICE", "ONE_SHOT": "TEMPI_DATATYPE_ONESHOT",
              "STAGED": "TEMPI_DATATYPE_STAGED"}
+    policies = [("DEVICE", (knobs["DEVICE"], None)), ("ONE_SHOT", (knobs["ONE_SHOT"], None)),
+                ("STAGED", (knobs["STAGED"], None)), ("learned", (None, "learned")),
+                ("table", (None, "table")), ("fixed", (None, "heuristic"))]
 
     def set_env(method_var=None, dispatch=None):
         for v in knobs.values():
@@ -654,46 +934,100 @@ def sendrecv_bench(torch, mpi, reps=2):
         assert (e1, e2) == (0, 0), _lib.last_error()
         assert mpi.Wait(rr)[0] == 0 and mpi.Wait(rs)[0] == 0, _lib.last_error()
 
+    host_write = host_write_gbs(torch, lib)
     rows = []
     for label, make, count in objs:
         t0 = make()
         lbext = mpi.Type_get_extent(t0)[1]
+        size = int(mpi.Type_size(t0)) * count
         src = torch.randint(0, 256, (lbext * count,), dtype=torch.uint8, device="cuda")
         dst = torch.zeros_like(src)
-        times, chosen = {}, {}
-        for policy, (var, disp) in [("DEVICE", (knobs["DEVICE"], None)),
-                                    ("ONE_SHOT", (knobs["ONE_SHOT"], None)),
-                                    ("STAGED", (knobs["STAGED"], None)),
-                                    ("learned", (None, "learned")),
-                                    ("table", (None, "table")),
-                                    ("fixed", (None, "heuristic"))]:
-            set_env(var, disp)
-            t = make()  # a fresh type per policy: no cached choice carries over
-            assert mpi.Type_commit(t) == 0
-            counts0 = {k: _lib.counter("send_" + k) for k in ("device", "oneshot", "staged")}
-            round_trip(t, count, src, dst)  # warm-up (and the policy's choice)
-            torch.cuda.synchronize()
-            t1 = _t.perf_counter()
-            for _ in range(reps):
+        n_reps = reps if size < (256 << 20) else max(3, reps // 4)
+        times = {name: [] for name, _ in policies}
+        chosen = {}
+        for rep in range(n_reps):
+            k = rep % len(policies)
+            for name, (var, disp) in policies[k:] + policies[:k]:
+                set_env(var, disp)
+                t = make()  # a fresh type: no cached choice carries over
+                assert mpi.Type_commit(t) == 0
+                round_trip(t, count, src, dst)  # untimed: the policy's choice, warm slabs
+                counts0 = {m: _lib.counter("send_" + m) for m in ("device", "oneshot", "staged")}
+                torch.cuda.synchronize()
+                t1 = _t.perf_counter()
                 round_trip(t, count, src, dst)
-            times[policy] = 1e6 * (_t.perf_counter() - t1) / reps
-            after = {k: _lib.counter("send_" + k) for k in ("device", "oneshot", "staged")}
-            chosen[policy] = [k for k in after if after[k] != counts0[k]]
-            mpi.Type_free(t)
+                times[name].append(1e6 * (_t.perf_counter() - t1))
+                after = {m: _lib.counter("send_" + m) for m in ("device", "oneshot", "staged")}
+                chosen[name] = [m for m in after if after[m] != counts0[m]]
+                mpi.Type_free(t)
         set_env()
-        best = min(times[m] for m in ("DEVICE", "ONE_SHOT", "STAGED"))
-        rows.append({"object": label, "bytes": int(mpi.Type_size(t0)) * count,
-                     **{k + "_us": round(v, 1) for k, v in times.items()},
-                     "best": min(("DEVICE", "ONE_SHOT", "STAGED"), key=lambda m: times[m]),
-                     "learned_pick": chosen.get("learned"), "table_pick": chosen.get("table"),
-                     "learned_regret": round(times["learned"] / best - 1, 4),
-                     "table_regret": round(times["table"] / best - 1, 4),
-                     "fixed_regret": round(times["fixed"] / best - 1, 4)})
+        med = {name: statistics.median(v) for name, v in times.items()}
+        best = min(med[m] for m in ("DEVICE", "ONE_SHOT", "STAGED"))
+        row = {"object": label, "bytes": size, "reps": n_reps,
+               **{k + "_us": round(v, 1) for k, v in med.items()},
+               "best": min(("DEVICE", "ONE_SHOT", "STAGED"), key=lambda m: med[m]),
+               "learned_pick": chosen.get("learned"), "table_pick": chosen.get("table"),
+               "learned_regret": round(med["learned"] / best - 1, 4),
+               "table_regret": round(med["table"] / best - 1, 4),
+               "fixed_regret": round(med["fixed"] / best - 1, 4)}
+        os_ = oneshot_pack_gbs(torch, lib, mpi, make(), count, src)
+        if os_ is not None:
+            row["oneshot_pack_gbs"] = round(os_, 2)
+            row["oneshot_pack_of_host_write"] = round(os_ / host_write, 3)
+        rows.append(row)
         del src, dst
     tot = {p: sum(r[p + "_us"] for r in rows) for p in ("learned", "table", "fixed")}
     best_tot = sum(min(r[m + "_us"] for m in ("DEVICE", "ONE_SHOT", "STAGED")) for r in rows)
-    return {"objects": rows,
+    return {"objects": rows, "host_write_gbs": round(host_write, 2),
+            "timing": "host wall clock per round trip, median over repetitions with the "
+                      "policy order rotated each repetition",
             "total_regret": {p: round(v / best_tot - 1, 4) for p, v in tot.items()}}
+
+
+def host_write_gbs(torch, lib, nbytes=256 << 20, reps=5):
+    """GB/s of a kernel writing pinned host memory: tempi_pack of a
+    contiguous 256 MiB type from device memory into a pinned host buffer."""
+    from tempi_b200 import _lib
+
+    d = _lib.Desc.make(0, nbytes, nbytes, [], [])
+    src = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    dst = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    cfg = _lib.Config(1, 16, 256, 0, 0, 0)
+    s = torch.cuda.Stream()
+    fn = lambda: _lib.check(lib.tempi_pack(ctypes.byref(d), src.data_ptr(), 1, dst.data_ptr(),
+                                           ctypes.byref(cfg), s.cuda_stream))
+    fn()
+    ms = time_events(torch, s, fn, reps)
+    del src, dst
+    return nbytes / ms / 1e6
+
+
+def oneshot_pack_gbs(torch, lib, mpi, t, count, src, reps=5):
+    """GB/s (packed bytes per second) of the pack a ONE_SHOT send runs: the
+    kernel the interposer picks for a pinned host packed buffer, writing
+    into mapped pinned host memory."""
+    from tempi_b200 import _lib
+
+    assert mpi.Type_commit(t) == 0
+    err, d = mpi.describe(t)
+    if err:
+        mpi.Type_free(t)
+        return None
+    n = d.size * count
+    host = torch.empty(n, dtype=torch.uint8).pin_memory()
+    pc, uc, mi = ctypes.c_int(-1), ctypes.c_int(-1), ctypes.c_int(0)
+    _lib.check(lib.tempi_dispatch_choose(ctypes.byref(d), count, 0, 1, 0, ctypes.byref(pc),
+                                         ctypes.byref(uc), ctypes.byref(mi), None, None))
+    cfg = _lib.Config(*_lib.CANDIDATE_CONFIGS[pc.value]) if pc.value >= 0 else None
+    s = torch.cuda.Stream()
+    fn = lambda: _lib.check(lib.tempi_pack(ctypes.byref(d), src.data_ptr(), count,
+                                           host.data_ptr(), ctypes.byref(cfg) if cfg else None,
+                                           s.cuda_stream))
+    fn()
+    ms = time_events(torch, s, fn, reps)
+    mpi.Type_free(t)
+    del host
+    return n / ms / 1e6
 
 
 def dispatch_sample(torch, n=200, seed=777):
@@ -867,14 +1201,20 @@ def run_ours(args):
         return
     side = torch.cuda.Stream()
     table = kernel_table(torch, sw, side, lib)
+    empty_ms = empty_kernel_events(torch, sw, side)
     total_t = sum(r["pack_ms"] + r["unpack_ms"] for r in table)
     top = max(table, key=lambda r: r["pack_ms"])
     peak, peak_kind = measured_peaks()
-    achieved = top["pack_gbs"]
+    # the dominant kernel again, launched back to back between one event
+    # pair: its inputs (typed and packed) are larger than the L2, so every
+    # launch streams from DRAM, and the event pair's own cost is spread over
+    # the launches
+    top_ms = dominant_back_to_back(torch, sw, side, lib, top["label"])
+    achieved = 2 * top["packed_bytes"] / top_ms / 1e6
     # the single-GPU characterisations run at N = 1 only: they would keep
     # the other ranks waiting at the final barrier
     solo = rank == 0 and world == 1
-    halo_res = halo_bench(torch, side) if solo else None
+    halo_res = halo_bench(torch, sw, side) if solo else None
     if halo_res is not None:
         halo_res["exchange"] = halo_exchange_bench(torch, side)
     # end to end: every rank at once, the whole job's rate from the slowest
@@ -907,6 +1247,9 @@ def run_ours(args):
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/traffic.txt",
             "share_of_kernel_time": round(top["pack_ms"] / total_t, 3),
             "alg_bytes_per_launch": 2 * top["packed_bytes"],
+            "launch_us": round(1e3 * top_ms, 2),
+            "timing": "10 back-to-back launches between one CUDA event pair on the launching "
+                      "stream (inputs 512 MiB, larger than L2), median of 5",
         },
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
@@ -916,8 +1259,19 @@ def run_ours(args):
         "type_commit": commit_res,
         "sendrecv": send_res,
         "dispatch": disp_res,
-        "sweep": [{"p": r["label"], "k": r["kernel"], "pack_gbs": round(r["pack_gbs"], 1),
-                   "unpack_gbs": round(r["unpack_gbs"], 1)} for r in table],
+        "sweep": [sweep_row(r, peak) for r in table],
+        "sweep_notes": {
+            "pack_gbs/unpack_gbs": "one launch of the kernel MPI_Pack/MPI_Unpack runs (the "
+                                   "learned pick), L2 flushed first, CUDA events around it: "
+                                   "includes the event pair and the launch's fixed cost",
+            "empty_kernel_us": round(1e3 * empty_ms, 2),
+            "kernel_gbs": "ncu in-kernel duration of the same launch (profiles/kernel_times.txt)",
+            "line_bound": "fraction of the copy peak the layout's unavoidable DRAM traffic "
+                          "allows (lines read by a pack, sectors written and merged by an unpack)",
+            "of_bound": "least in-kernel time (the larger of: empty kernel + line traffic at "
+                        "the peak; a one-load gather of scattered lines) / measured in-kernel "
+                        "time",
+        },
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_budget)
@@ -926,6 +1280,124 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+LAUNCH_LIST_REPS = 3
+GATHER_ROWS, GATHER_STRIDE = 16384, 4096
+
+
+def launch_list_order():
+    """The launches of --launch-list, in order: an empty kernel, then each
+    sweep point's pack and unpack kernel, LAUNCH_LIST_REPS times over."""
+    order = []
+    for _ in range(LAUNCH_LIST_REPS):
+        order += [("empty", "-"), ("gather", "-")]
+        for label, *_ in sweep_points():
+            order += [(label, "pack"), (label, "unpack")]
+    return order
+
+
+def run_launch_list(args):
+    """For an ncu launch list (gpu__time_duration, one pass): the kernel
+    MPI_Pack / MPI_Unpack run for every sweep point at its benchmark
+    incount, one launch at a time with the L2 flushed before each, after an
+    empty kernel; see --summarize-launches."""
+    import torch
+
+    from tempi_b200 import _lib, mpi
+
+    assert mpi.Init() == 0
+    lib = _lib.tempi()
+    sw = GpuSweep(torch, mpi, torch.device("cuda", 0))
+    stream = torch.cuda.Stream()
+    s = stream.cuda_stream
+    plans = {}
+    for p in sw.pts:  # every cost-model inference happens here, before the list
+        err, d = mpi.describe(p["t"])
+        assert err == 0
+        plans[p["label"]] = (p, d, learned_configs(lib, d, p["incount"]))
+    torch.cuda.synchronize()
+    names = []
+    for label, direction in launch_list_order():
+        sw.flush_l2(stream)
+        if label == "empty":
+            assert driver().tempi_bench_empty(s) == 0
+            names.append("empty")
+        elif label == "gather":  # one scattered line per thread: 16,384 rows 4 KiB apart
+            assert GATHER_ROWS * GATHER_STRIDE <= sw.src2.numel()
+            assert driver().tempi_bench_gather(sw.src2.data_ptr(), GATHER_STRIDE, GATHER_ROWS,
+                                               sw.packed.data_ptr(), s) == 0
+            names.append("gather")
+        else:
+            p, d, (cp, cu) = plans[label]
+            n = p["incount"]
+            if direction == "pack":
+                _lib.check(lib.tempi_pack(ctypes.byref(d), p["src"].data_ptr(), n,
+                                          sw.packed.data_ptr(), ctypes.byref(cp) if cp else None, s))
+            else:
+                _lib.check(lib.tempi_unpack(ctypes.byref(d), sw.packed.data_ptr(), n,
+                                            p["dst"].data_ptr(), ctypes.byref(cu) if cu else None, s))
+            names.append(lib.tempi_last_kernel().decode())
+        stream.synchronize()
+    print(json.dumps({"launch_list": len(names), "kernels": names[:2 + 2 * len(sw.pts)]}))
+
+
+def summarize_launches(path, out_txt=None):
+    """Per sweep point and direction, the median in-kernel time of the
+    kernels --launch-list ran, from ncu's CSV (gpu__time_duration.sum),
+    against the measured copy peak and the point's line-traffic bound.
+    Prints a markdown table; writes `out_txt` (point direction us) when
+    given."""
+    import csv
+
+    rows = list(csv.reader(open(path)))
+    hi = next(i for i, r in enumerate(rows) if "Kernel Name" in r)
+    h = rows[hi]
+    ki, vi, ui = h.index("Kernel Name"), h.index("Metric Value"), h.index("Metric Unit")
+    seq = []
+    for r in rows[hi + 1:]:
+        if len(r) <= vi or r[h.index("Metric Name")] != "gpu__time_duration.sum":
+            continue
+        name = r[ki]
+        if "read_all" in name or "k_mlp" in name or "Fill" in name or "fill" in name:
+            continue
+        v = float(r[vi].replace(",", ""))
+        scale = {"nsecond": 1e-3, "usecond": 1.0, "msecond": 1e3}.get(r[ui], 1e-3)
+        seq.append((name, v * scale))
+    order = launch_list_order()
+    if len(seq) != len(order):
+        raise SystemExit(f"{len(seq)} kernels in the CSV, {len(order)} expected")
+    by = {}
+    for (label, direction), (name, us) in zip(order, seq):
+        by.setdefault((label, direction), []).append((name, us))
+    peak, kind = measured_peaks()
+    pts = {p[0]: p for p in sweep_points()}
+    empty = statistics.median(us for _, us in by[("empty", "-")])
+    gather = statistics.median(us for _, us in by[("gather", "-")])
+    lines = ["| point | dir | kernel | packed | in-kernel us | GB/s | of peak | line bound us "
+             "| bound us | of that bound |", "|" + "---|" * 10]
+    txt = [f"# point direction in_kernel_us  (ncu gpu__time_duration.sum, median of "
+           f"{LAUNCH_LIST_REPS}; empty kernel {empty:.2f} us; one-load gather {gather:.2f} us)"]
+    for label, sizes, subs, starts, n in sweep_points():
+        size = 4 * int(np.prod(subs)) * n
+        for u, direction in enumerate(("pack", "unpack")):
+            ks = by[(label, direction)]
+            us = statistics.median(x for _, x in ks)
+            kname = ks[0][0].split("(")[0].replace("void ", "").replace("tempi::", "")
+            tr = line_traffic(sizes, subs, starts, n, u)
+            lb = tr / peak / 1e3
+            gbs = 2 * size / us / 1e3
+            bound = point_bound(empty, gather, tr, peak)
+            lines.append(f"| {label} | {direction} | `{kname}` | {size / 2**20:.3g} MiB | "
+                         f"{us:.2f} | {gbs:.0f} | {gbs / peak:.3f} | {lb:.2f} | "
+                         f"{bound:.2f} | {bound / us:.2f} |")
+            txt.append(f"{label} {direction} {us:.3f}")
+    print(f"empty kernel: {empty:.2f} us, one-load gather of {GATHER_ROWS} rows: {gather:.2f} us "
+          f"in-kernel (medians); peak {peak} GB/s ({kind})")
+    print("\n".join(lines))
+    if out_txt:
+        with open(out_txt, "w") as f:
+            f.write("\n".join(txt) + "\n")
 
 
 def run_profile(args):
@@ -1158,8 +1630,18 @@ def main():
                     help="measure the host-link rates and exit")
     ap.add_argument("--profile-exchange", action="store_true",
                     help="run only the fused halo-exchange kernel (for ncu)")
+    ap.add_argument("--launch-list", action="store_true",
+                    help="each sweep point's kernels once per pass, L2 flushed (for an ncu "
+                         "launch list)")
+    ap.add_argument("--summarize-launches", default=None, metavar="CSV",
+                    help="per-point in-kernel times from the ncu CSV of --launch-list")
+    ap.add_argument("--out", default=None, help="with --summarize-launches: a table file")
     args = ap.parse_args()
-    if args.host_link:
+    if args.summarize_launches:
+        summarize_launches(args.summarize_launches, args.out)
+    elif args.launch_list:
+        run_launch_list(args)
+    elif args.host_link:
         run_host_link(args)
     elif args.profile_exchange:
         run_profile_exchange(args)

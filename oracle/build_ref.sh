@@ -1,7 +1,9 @@
 #!/bin/sh
 # ORACLE -- builds the reference's packer kernels from the reference sources
 # (read where they lie, never copied) into oracle/_ref/libref_pack.so.
-# Needs the reference tree; the built .so then travels with the repository.
+# Needs the reference tree (TEMPI_REFERENCE, else the checkout this recipe was
+# written against); without it the recipe does nothing and exits 0.  The
+# built .so then travels with the repository.
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
 REF=${TEMPI_REFERENCE:-/root/reference}

@@ -30,6 +30,17 @@ __global__ void read_all(const uint4 *__restrict__ buf, size_t n,
 
 unsigned *g_sink = nullptr;
 
+__global__ void k_bench_empty() {}
+
+// one 4-B load per thread from rows `stride` bytes apart, stored densely:
+// the least work a kernel that reads scattered DRAM lines can do
+__global__ void k_bench_gather(const char *__restrict__ base, long long stride,
+                               int rows, uint32_t *__restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < rows)
+    out[t] = __ldg(reinterpret_cast<const uint32_t *>(base + t * stride));
+}
+
 } // namespace
 
 extern "C" {
@@ -62,6 +73,24 @@ int tempi_bench_copy2d(void *dst, size_t dpitch, const void *src, size_t spitch,
     return 2;
   }
   return 0;
+}
+
+// One launch of an empty kernel on `stream`: the fixed cost of any launch,
+// measured beside the pack kernels (by CUDA events, or by ncu's duration).
+int tempi_bench_empty(void *stream) {
+  k_bench_empty<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>();
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// k_bench_gather over `rows` rows of `base`; the caller keeps
+// (rows - 1) * stride + 4 bytes of `base` and 4 * rows bytes of `out` valid
+int tempi_bench_gather(const void *base, long long stride, int rows, void *out,
+                       void *stream) {
+  if (rows <= 0 || stride < 4)
+    return 1;
+  k_bench_gather<<<(rows + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const char *>(base), stride, rows, static_cast<uint32_t *>(out));
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
 int tempi_bench_flush(void *buf, size_t bytes, void *stream) {

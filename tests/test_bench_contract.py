@@ -6,6 +6,8 @@ import os
 import subprocess
 import sys
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -41,3 +43,72 @@ def test_reference_arm_json_line():
 
 def test_reference_arm_other_ranks_are_silent():
     assert _run({"RANK": "1", "WORLD_SIZE": "2"}) == []
+
+
+def test_line_traffic_model():
+    """The line-traffic bound of a sweep point, by hand: 64-B rows at byte
+    120 of a 128-B line touch two lines (a pack reads 256 B per row and
+    writes 64), and three 32-B sectors (an unpack reads 64 packed bytes and
+    writes three sectors)."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    sizes, subs, starts = [256, 256, 256], [256, 256, 16], [0, 0, 30]
+    rows = 256 * 256
+    assert bench.line_traffic(sizes, subs, starts, 1, 0) == rows * (256 + 64)
+    assert bench.line_traffic(sizes, subs, starts, 1, 1) == rows * (64 + 32 * 3)
+    # a full subarray is one contiguous run per object: read and write it once
+    full = bench.line_traffic(sizes, sizes, [0, 0, 0], 4, 0)
+    assert full == 2 * 4 * 4 * 256 ** 3
+    # every point's bound is at most the copy peak, and the contiguous ones reach it
+    for label, sz, sb, st, n in bench.sweep_points():
+        alg = 2 * 4 * int(np.prod(sb)) * n
+        for u in (0, 1):
+            t = bench.line_traffic(sz, sb, st, n, u)
+            assert t >= alg, (label, u)
+            if label in ("2d_i1024", "3d_i256"):
+                assert t == alg
+
+
+def test_launch_list_summary(tmp_path):
+    """--summarize-launches reads ncu's CSV of a --launch-list run (launches
+    in the order launch_list_order gives, flush and inference kernels in
+    between) into per-point in-kernel times."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    header = ["ID", "Process ID", "Process Name", "Host Name", "Kernel Name", "Context",
+              "Stream", "Block Size", "Grid Size", "Device", "CC", "Section Name",
+              "Metric Name", "Metric Unit", "Metric Value"]
+    lines = [",".join(f'"{h}"' for h in header)]
+    k = 0
+
+    def add(name, ns):
+        nonlocal k
+        row = [str(k), "1", "python", "h", name, "1", "7", "(256, 1, 1)", "(148, 1, 1)", "0",
+               "10.0", "Command line profiler metrics", "gpu__time_duration.sum", "nsecond",
+               f"{ns:,}"]
+        lines.append(",".join(f'"{x}"' for x in row))
+        k += 1
+
+    add("tempi::k_mlp_predict(const float *, const float *, int, float *)", 9000)
+    for i, (label, direction) in enumerate(bench.launch_list_order()):
+        add("(anonymous namespace)::read_all(const uint4 *, unsigned long, unsigned int *)", 80000)
+        ns = {"empty": 1900, "gather": 3500}.get(label, 3000 + 10 * i)
+        name = {"empty": "(anonymous namespace)::k_bench_empty()",
+                "gather": "(anonymous namespace)::k_bench_gather(const char *, long long, int, "
+                          "unsigned int *)"}.get(
+            label, "void tempi::k_words<4, 1, 0>(char *, char *, tempi::Geometry)")
+        add(name, ns)
+    csv = tmp_path / "launches.csv"
+    csv.write_text("==PROF== Connected\n" + "\n".join(lines) + "\n")
+    out = tmp_path / "kernel_times.txt"
+    bench.summarize_launches(str(csv), str(out))
+    txt = out.read_text().splitlines()
+    assert "empty kernel 1.90 us" in txt[0] and "gather 3.50 us" in txt[0]
+    got = dict(((l.split()[0], l.split()[1]), float(l.split()[2])) for l in txt[1:])
+    assert len(got) == 2 * len(bench.sweep_points())
+    order = bench.launch_list_order()
+    per = len(order) // bench.LAUNCH_LIST_REPS
+    i = order.index(("2d_i1", "pack"))
+    assert got[("2d_i1", "pack")] == (3000 + 10 * (i + per)) / 1e3  # the median of three

@@ -164,3 +164,97 @@ def test_reference_kernels_misbehave_where_documented(cuda, mpi_init, ref):
     ty = H.vector(64, 8, 12, H.named()).commit()
     err, d = mpi.describe(ty.h)
     assert err == 0 and d.align == 4
+
+
+def test_reference_kernels_on_the_sweep(cuda, mpi_init, ref):
+    """Every point of the benchmark's strided sweep at its benchmark incount:
+    the reference's packer (its pack_2d/pack_3d kernels, or for a contiguous
+    type its Packer1D's cudaMemcpyAsync) against the kernel the interposer
+    runs (the learned pick), on the same device buffers.  Both write the same
+    bytes; both are timed alike (the L2 flushed before every launch, CUDA
+    events around it, median of 5; event pair and launch overhead included in
+    both).  The sweep's pitches and extents are
+    multiples of 16 B and its buffers 256-B aligned, so the reference's word
+    size (chosen from block length and start only) is safe on every point.
+    Results go to $TEMPI_RESULTS_DIR/ref_kernels_sweep.json when set."""
+    import statistics
+    import sys
+
+    import torch
+
+    sys.path.insert(0, ROOT)
+    from bench import learned_configs, sweep_points
+
+    lib = _lib.tempi()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    rows = []
+    for label, sizes, subs, starts, incount in sweep_points():
+        o = T.subarray(sizes, subs, starts, T.ORDER_C, T.FLOAT)
+        sb = R.canonicalize(o)
+        t = mpi.Type_create_subarray(sizes, subs, starts, mpi.ORDER_C, mpi.FLOAT)
+        assert mpi.Type_commit(t) == 0
+        err, d = mpi.describe(t)
+        assert err == 0
+        cp, cu = learned_configs(lib, d, incount)
+        src = torch.randint(0, 256, (o.extent * incount,), dtype=torch.uint8, device="cuda")
+        p_ref = torch.zeros(o.size * incount, dtype=torch.uint8, device="cuda")
+        p_tempi = torch.zeros_like(p_ref)
+        u_ref = torch.full_like(src, 0xAA)
+        u_tempi = torch.full_like(src, 0xAA)
+        contiguous = sb.ndims <= 1
+
+        def launch(who, unpack):
+            if who == "tempi":
+                if unpack:
+                    _lib.check(lib.tempi_unpack(ctypes.byref(d), p_tempi.data_ptr(), incount,
+                                                u_tempi.data_ptr(), ctypes.byref(cu) if cu else None,
+                                                None))
+                else:
+                    _lib.check(lib.tempi_pack(ctypes.byref(d), src.data_ptr(), incount,
+                                              p_tempi.data_ptr(), ctypes.byref(cp) if cp else None,
+                                              None))
+            elif contiguous:  # Packer1D: one cudaMemcpyAsync of the packed bytes
+                off = sb.start if sb.ndims == 1 else 0
+                if unpack:
+                    u_ref[off: off + p_ref.numel()].copy_(p_ref)
+                else:
+                    p_ref.copy_(src[off: off + p_ref.numel()])
+            else:
+                assert ref_launch(ref, sb, unpack, (u_ref if unpack else src).data_ptr(),
+                                  p_ref.data_ptr(), incount) == 0
+
+        times = {}
+        for who in ("reference", "tempi"):
+            for unpack in (0, 1):
+                launch(who, unpack)
+                ts = []
+                for _ in range(5):
+                    flush.fill_(1)  # evict the L2, then read back so its lines are clean
+                    flush.view(torch.int64).sum()
+                    e0, e1 = _events()
+                    e0.record()
+                    launch(who, unpack)
+                    e1.record()
+                    e1.synchronize()
+                    ts.append(e0.elapsed_time(e1))
+                times[(who, unpack)] = statistics.median(ts)
+        torch.cuda.synchronize()
+        assert torch.equal(p_ref, p_tempi), label
+        assert torch.equal(u_ref, u_tempi), label
+        mpi.Type_free(t)
+        alg = 2 * o.size * incount
+        rows.append({
+            "point": label, "incount": incount, "packed_bytes": o.size * incount,
+            "reference": "Packer1D cudaMemcpyAsync" if contiguous else f"pack_{sb.ndims}d",
+            "ref_pack_gbs": round(alg / times[("reference", 0)] / 1e6, 1),
+            "ref_unpack_gbs": round(alg / times[("reference", 1)] / 1e6, 1),
+            "tempi_pack_gbs": round(alg / times[("tempi", 0)] / 1e6, 1),
+            "tempi_unpack_gbs": round(alg / times[("tempi", 1)] / 1e6, 1),
+            "pack_speedup": round(times[("reference", 0)] / times[("tempi", 0)], 2),
+            "unpack_speedup": round(times[("reference", 1)] / times[("tempi", 1)], 2),
+        })
+    print(json.dumps(rows, indent=1))
+    out = os.environ.get("TEMPI_RESULTS_DIR", "")
+    if out and os.path.isdir(out):
+        with open(os.path.join(out, "ref_kernels_sweep.json"), "w") as f:
+            json.dump(rows, f, indent=1)
