@@ -455,7 +455,7 @@ def sweep_row(r, peak):
     out = {"p": r["label"], "k": r["kernel"], "ku": r["ukernel"],
            "pack_gbs": round(r["pack_gbs"], 1), "unpack_gbs": round(r["unpack_gbs"], 1),
            "line_bound": [round(x, 3) for x in r["line_bound"]]}
-    empty, gather = KERNEL_FLOORS_US
+    empty, gather, _ = KERNEL_FLOORS_US
     kg, ob = [], []
     for u, direction in enumerate(("pack", "unpack")):
         us = r.get(direction + "_kernel_us")
@@ -471,9 +471,9 @@ def sweep_row(r, peak):
     return out
 
 
-# in-kernel times of the empty kernel and the one-load gather in the
-# committed launch list (ncu)
-KERNEL_FLOORS_US = [None, None]
+# in-kernel times of the empty kernel, the one-load gather and one scattered
+# line in the committed launch list (ncu)
+KERNEL_FLOORS_US = [None, None, None]
 
 
 def dominant_back_to_back(torch, sw, stream, lib, label, k=10, reps=5):
@@ -518,6 +518,8 @@ def kernel_times_from_profiles():
                 KERNEL_FLOORS_US[0] = float(line.split("empty kernel")[1].split()[0])
                 if "gather" in line:
                     KERNEL_FLOORS_US[1] = float(line.split("gather")[1].split()[0])
+                if "scattered line" in line:
+                    KERNEL_FLOORS_US[2] = float(line.split("scattered line")[1].split()[0]) / 1e6
             elif len(f) >= 3 and not line.startswith("#"):
                 out[(f[0], f[1])] = float(f[2])
     return out
@@ -1033,35 +1035,45 @@ def oneshot_pack_gbs(torch, lib, mpi, t, count, src, reps=5):
 def dispatch_sample(torch, n=200, seed=777):
     """Held-out sample for the learned kernel-configuration choice: fresh
     random layouts (a seed the model never saw), every eligible candidate
-    timed, the learned pick and the fixed rules against the best."""
+    timed, the learned pick and the fixed rules against the best.  Every
+    layout is measured twice: the second measurement shows how often the
+    first one's own fastest candidate stays within 5 % of the fastest when
+    timed again (the noise ceiling of the within-5 % figure)."""
     from tempi_b200 import _lib
     from tempi_b200 import dispatch_train as DT
 
     lib = _lib.tempi()
     rng = np.random.default_rng(seed)
     times = (ctypes.c_float * DT.N_MEAS)()
-    learned, fixed, best, where = [], [], [], []
+    times2 = (ctypes.c_float * DT.N_MEAS)()
+    learned, fixed, best, where, rep_best, rep_self = [], [], [], [], [], []
     t0 = time.time()
-    while len(best) < n and time.time() - t0 < 60:
+    while len(best) < n and time.time() - t0 < 90:
         d, incount, th, ph = DT.random_layout(rng)
         if DT.span_of(d, incount) > (2 << 30) or (th and DT.span_of(d, incount) > (16 << 20)):
             continue
         size = d.size * incount
-        reps = 3 if size < (1 << 20) else 2 if size < (64 << 20) else 1
+        reps = 8 if size < (1 << 20) else 3 if size < (64 << 20) else 1
         _lib.check(lib.tempi_measure(ctypes.byref(d), incount, int(th), int(ph), 1, reps, times))
+        _lib.check(lib.tempi_measure(ctypes.byref(d), incount, int(th), int(ph), 1, reps, times2))
         pc, uc, mi = ctypes.c_int(-1), ctypes.c_int(-1), ctypes.c_int(0)
         if lib.tempi_dispatch_choose(ctypes.byref(d), incount, int(th), int(ph), 0,
                                      ctypes.byref(pc), ctypes.byref(uc), ctypes.byref(mi),
                                      None, None):
             return {"error": _lib.last_error()}
         t = np.frombuffer(times, np.float32)
-        tp = t[DT.PACK:DT.PACK + DT.N_CFG]
-        tu = t[DT.UNPACK:DT.UNPACK + DT.N_CFG]
+        t2 = np.frombuffer(times2, np.float32)
+        tp, tu = t[DT.PACK:DT.PACK + DT.N_CFG], t[DT.UNPACK:DT.UNPACK + DT.N_CFG]
+        tp2, tu2 = t2[DT.PACK:DT.PACK + DT.N_CFG], t2[DT.UNPACK:DT.UNPACK + DT.N_CFG]
         best.append(float(np.nanmin(tp) + np.nanmin(tu)))
         learned.append(float(tp[pc.value] + tu[uc.value]))
         fixed.append(float(t[DT.FIXED_PACK] + t[DT.FIXED_UNPACK]))
+        # the first measurement's own picks, timed again
+        rep_self.append(float(tp2[int(np.nanargmin(tp))] + tu2[int(np.nanargmin(tu))]))
+        rep_best.append(float(np.nanmin(tp2) + np.nanmin(tu2)))
         where.append((d.as_dict(), incount, bool(th), bool(ph), pc.value, uc.value))
     L, F, B = map(np.array, (learned, fixed, best))
+    RS, RB = np.array(rep_self), np.array(rep_best)
     worst = [{"us_learned": round(float(L[i]), 1), "us_best": round(float(B[i]), 1),
               "layout": where[i][0], "incount": where[i][1], "typed_host": where[i][2],
               "packed_host": where[i][3], "picks": where[i][4:]}
@@ -1071,7 +1083,10 @@ def dispatch_sample(torch, n=200, seed=777):
             "fixed_rules_total_regret": round(float(F.sum() / B.sum() - 1), 4),
             "learned_within_5pct": round(float(np.mean(L <= 1.05 * B)), 3),
             "learned_mean_regret": round(float(np.mean(L / B - 1)), 4),
+            "exhaustive_repeat_within_5pct": round(float(np.mean(RS <= 1.05 * RB)), 3),
+            "exhaustive_repeat_total_regret": round(float(RS.sum() / RB.sum() - 1), 4),
             "exhaustive_total_us": round(float(B.sum()), 1),
+            "reps": "8 back-to-back launches per candidate under 1 MiB, 3 under 64 MiB, else 1",
             "largest_losses": worst}
 
 
@@ -1284,6 +1299,7 @@ def run_ours(args):
 
 LAUNCH_LIST_REPS = 3
 GATHER_ROWS, GATHER_STRIDE = 16384, 4096
+BIG_GATHER_ROWS, BIG_GATHER_STRIDE = 262144, 1024
 
 
 def launch_list_order():
@@ -1291,7 +1307,7 @@ def launch_list_order():
     sweep point's pack and unpack kernel, LAUNCH_LIST_REPS times over."""
     order = []
     for _ in range(LAUNCH_LIST_REPS):
-        order += [("empty", "-"), ("gather", "-")]
+        order += [("empty", "-"), ("gather", "-"), ("gather_big", "-")]
         for label, *_ in sweep_points():
             order += [(label, "pack"), (label, "unpack")]
     return order
@@ -1328,6 +1344,12 @@ def run_launch_list(args):
             assert driver().tempi_bench_gather(sw.src2.data_ptr(), GATHER_STRIDE, GATHER_ROWS,
                                                sw.packed.data_ptr(), s) == 0
             names.append("gather")
+        elif label == "gather_big":  # 262,144 rows 1 KiB apart: the scattered-line rate
+            assert BIG_GATHER_ROWS * BIG_GATHER_STRIDE <= sw.src3.numel()
+            assert 4 * BIG_GATHER_ROWS <= sw.packed.numel()
+            assert driver().tempi_bench_gather(sw.src3.data_ptr(), BIG_GATHER_STRIDE,
+                                               BIG_GATHER_ROWS, sw.packed.data_ptr(), s) == 0
+            names.append("gather_big")
         else:
             p, d, (cp, cu) = plans[label]
             n = p["incount"]
@@ -1339,7 +1361,7 @@ def run_launch_list(args):
                                             p["dst"].data_ptr(), ctypes.byref(cu) if cu else None, s))
             names.append(lib.tempi_last_kernel().decode())
         stream.synchronize()
-    print(json.dumps({"launch_list": len(names), "kernels": names[:2 + 2 * len(sw.pts)]}))
+    print(json.dumps({"launch_list": len(names), "kernels": names[:3 + 2 * len(sw.pts)]}))
 
 
 def summarize_launches(path, out_txt=None):
@@ -1374,10 +1396,12 @@ def summarize_launches(path, out_txt=None):
     pts = {p[0]: p for p in sweep_points()}
     empty = statistics.median(us for _, us in by[("empty", "-")])
     gather = statistics.median(us for _, us in by[("gather", "-")])
+    line_us = (statistics.median(us for _, us in by[("gather_big", "-")]) - empty) / BIG_GATHER_ROWS
     lines = ["| point | dir | kernel | packed | in-kernel us | GB/s | of peak | line bound us "
              "| bound us | of that bound |", "|" + "---|" * 10]
     txt = [f"# point direction in_kernel_us  (ncu gpu__time_duration.sum, median of "
-           f"{LAUNCH_LIST_REPS}; empty kernel {empty:.2f} us; one-load gather {gather:.2f} us)"]
+           f"{LAUNCH_LIST_REPS}; empty kernel {empty:.2f} us; one-load gather {gather:.2f} us; "
+           f"scattered line {1e6 * line_us:.2f} ps)"]
     for label, sizes, subs, starts, n in sweep_points():
         size = 4 * int(np.prod(subs)) * n
         for u, direction in enumerate(("pack", "unpack")):
@@ -1392,7 +1416,8 @@ def summarize_launches(path, out_txt=None):
                          f"{us:.2f} | {gbs:.0f} | {gbs / peak:.3f} | {lb:.2f} | "
                          f"{bound:.2f} | {bound / us:.2f} |")
             txt.append(f"{label} {direction} {us:.3f}")
-    print(f"empty kernel: {empty:.2f} us, one-load gather of {GATHER_ROWS} rows: {gather:.2f} us "
+    print(f"empty kernel: {empty:.2f} us, one-load gather of {GATHER_ROWS} rows: {gather:.2f} us, "
+          f"one scattered line {1e6 * line_us:.2f} ps (gather of {BIG_GATHER_ROWS} rows) "
           f"in-kernel (medians); peak {peak} GB/s ({kind})")
     print("\n".join(lines))
     if out_txt:
@@ -1401,8 +1426,9 @@ def summarize_launches(path, out_txt=None):
 
 
 def run_profile(args):
-    """A small case for ncu: one sweep point's pack (or unpack) kernel,
-    launched --profile-reps times through tempi_pack/tempi_unpack."""
+    """A small case for ncu: one sweep point's pack (or unpack) kernel, the
+    one the learned dispatch picks, launched --profile-reps times through
+    tempi_pack/tempi_unpack."""
     import torch
 
     from tempi_b200 import _lib, mpi
@@ -1422,13 +1448,14 @@ def run_profile(args):
     dst = torch.zeros_like(src)
     packed = torch.zeros(d.size * n, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
+    cp, cu = learned_configs(lib, d, n)  # the kernels MPI_Pack / MPI_Unpack run
     for _ in range(args.profile_reps):
         if args.profile_unpack:
             _lib.check(lib.tempi_unpack(ctypes.byref(d), packed.data_ptr(), n, dst.data_ptr(),
-                                        None, None))
+                                        ctypes.byref(cu) if cu else None, None))
         else:
             _lib.check(lib.tempi_pack(ctypes.byref(d), src.data_ptr(), n, packed.data_ptr(),
-                                      None, None))
+                                      ctypes.byref(cp) if cp else None, None))
     torch.cuda.synchronize()
     print(json.dumps({"profile_point": label, "incount": n, "packed_bytes": d.size * n,
                       "kernel": lib.tempi_last_kernel().decode(),

@@ -24,6 +24,8 @@
         MPI_Neighbor_alltoallw
                           replaces reference src/neighbor_alltoallw.cpp:11-17
                           + src/internal/neighbor_alltoallw.cpp:19-85
+        MPI_Alltoallv     replaces reference src/alltoallv.cpp:14-66
+                          + src/internal/alltoallv_impl.cpp:21-258
 
       Signatures are those of include/symbols.hpp in the reference
       (PARAMS_MPI_* macros, lines 10-178).
@@ -136,6 +138,27 @@ int tempi_batch_launch(tempi_batch *b, void *stream);
 int tempi_batch_capture(tempi_batch *b, void *stream);
 int tempi_batch_replay(tempi_batch *b, void *stream);
 int tempi_batch_destroy(tempi_batch *b);
+
+/* The batch autotuner.  A batch launch is one kernel over warp chunks; its
+   choices are the launch shape (threads per block 128/256/512, blocks per
+   SM) and, per region class (class = 8 * log2(width) + min(7, log2(words
+   per row)): the proven vector width and the row length), the passes of a
+   warp over one chunk (1, 2 or 4: the chunk size).  tempi_batch_tune times
+   the batch on `stream` (`reps` launches per candidate, the L2 flushed
+   before each; it allocates and frees a flush buffer of twice the L2),
+   keeps the fastest choices for this batch, and remembers them for every
+   later batch with the same signature (the same region classes and sizes)
+   in this process and in TEMPI_CACHE_DIR/tempi_b200_batch_tune.txt.  It
+   drops a captured graph: capture again after tuning.  The reference has
+   no counterpart (it packs one object per launch). */
+int tempi_batch_tune(tempi_batch *b, void *stream, int32_t reps);
+/* The choices a batch launches with: threads per block, blocks per SM (0:
+   as many as fit), and for each region class present (ascending, at most
+   max_classes) its passes.  Returns the number of classes written, or a
+   negative TEMPI_ERR_* code. */
+int tempi_batch_config(const tempi_batch *b, int32_t *threads,
+                       int32_t *ctas_per_sm, int32_t *classes,
+                       int32_t *passes, int32_t max_classes);
 
 /* Batched exchange: every region is copied from one strided layout straight
    into another (typed -> typed, no packed buffer between them), all regions
@@ -279,9 +302,13 @@ const char *tempi_last_kernel(void);
    "lib_pack", "lib_unpack", "cached_types", "send_device", "send_oneshot",
    "send_staged", "send_lib", "recv_device", "recv_oneshot", "recv_staged",
    "recv_lib", "isend_managed", "irecv_managed", "dispatch_hit",
-   "dispatch_miss", "slab_hits", "slab_misses", "slab_bytes",
+   "dispatch_miss", "slab_hits", "slab_misses", "slab_bytes" (bytes of
+   slabs held from CUDA), "slab_live_bytes" (handed out), "slab_cached_bytes"
+   (kept for reuse, at most TEMPI_SLAB_CACHE_MB per memory space),
    "host_link_copies", "send_contig_staged", "recv_contig_staged",
-   "neighbor_fused", "neighbor_isir", "neighbor_lib", and "staged_timeouts"
+   "neighbor_fused", "neighbor_isir", "neighbor_lib", "alltoallv_staged",
+   "alltoallv_remote_first", "alltoallv_isir_staged",
+   "alltoallv_isir_remote_staged", "alltoallv_lib", and "staged_timeouts"
    (staged launches whose bounded waits gave up, as far as the host has seen:
    see tempi_staged_check); -1 for an unknown name */
 int64_t tempi_counter(const char *name);

@@ -175,13 +175,16 @@ _MPI_SIGS = {
                                        c_void_p, c_int, c_int]),
     "MPI_Neighbor_alltoallw": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                        c_void_p, c_void_p, c_void_p, c_int]),
+    "MPI_Alltoallv": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                              c_void_p, c_int, c_int]),
+    "MPI_Barrier": (c_int, [c_int]),
 }
 
 # the interposed entry points libtempi_b200.so must export
 INTERPOSED = [
     "MPI_Init", "MPI_Init_thread", "MPI_Finalize", "MPI_Type_commit",
     "MPI_Type_free", "MPI_Pack", "MPI_Unpack", "MPI_Send", "MPI_Recv",
-    "MPI_Isend", "MPI_Irecv", "MPI_Wait", "MPI_Neighbor_alltoallw",
+    "MPI_Isend", "MPI_Irecv", "MPI_Wait", "MPI_Neighbor_alltoallw", "MPI_Alltoallv",
 ]
 
 _TEMPI_SIGS = {

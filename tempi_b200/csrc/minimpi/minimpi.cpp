@@ -1,5 +1,8 @@
-// libminimpi: a self-only MPI library (world size 1) that stands in for the
-// system MPI, which does not exist on the machines this project runs on.
+// libminimpi: a small MPI library that stands in for the system MPI, which
+// does not exist on the machines this project runs on.  One process is world
+// size 1; several processes on one host form a larger world when each is
+// started with MINIMPI_SIZE, MINIMPI_RANK and a shared MINIMPI_DIR: the ranks
+// then connect by Unix-domain stream sockets in that directory, one per pair.
 //
 // Datatypes follow the MPI-3.1 type-map definitions (section 4.1): each
 // constructor describes a sequence of (displacement, basic type) entries in a
@@ -10,17 +13,34 @@
 // Point-to-point calls match in MPI order: a send goes to the earliest posted
 // receive that matches it, else it is buffered (eagerly, always) as an
 // unexpected message; a receive takes the earliest matching unexpected message.
-// With one rank and one thread, a blocking receive that has nothing to match
-// can never complete, so it returns MPI_ERR_OTHER instead of hanging.
+// A send to another rank is packed into host bytes and written to that rank's
+// socket; a stream per pair keeps messages between two ranks in order, as
+// MPI's non-overtaking rule needs.  Messages are read from the sockets
+// whenever a call makes progress (tests, waits, and a send blocked on a full
+// socket, so two ranks sending to each other never deadlock).  With one
+// rank, a blocking receive that has nothing to match can never complete, so
+// it returns MPI_ERR_OTHER instead of hanging; with several, it waits for at
+// most MINIMPI_TIMEOUT_S seconds (default 60) before it does the same.
 
 #include "mpi.h"
 
 #include <cuda_runtime.h>
 
+#include <fcntl.h>
+#include <poll.h>
+#include <sys/socket.h>
+#include <sys/stat.h>
+#include <sys/un.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <cerrno>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
+#include <thread>
 #include <ctime>
 #include <deque>
 #include <mutex>
@@ -255,6 +275,69 @@ bool is_device(const void *p) {
   return a.type == cudaMemoryTypeDevice;
 }
 
+// Every copy that touches GPU memory runs on the library's own stream and is
+// waited for before the call returns, so a completed send or receive has its
+// bytes in place for any later work on any stream.  (A device-to-device
+// cudaMemcpy returns before the copy is done, and the legacy stream it runs
+// on does not order work on non-blocking streams, such as the one a caller
+// unpacks a received buffer on.)
+int cuda_copy(void *dst, const void *src, size_t n) {
+  static cudaStream_t stream = nullptr;
+  if (n == 0)
+    return MPI_SUCCESS;
+  if (!stream && cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return MPI_ERR_OTHER;
+  }
+  if (cudaMemcpyAsync(dst, src, n, cudaMemcpyDefault, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    cudaGetLastError();
+    return MPI_ERR_OTHER;
+  }
+  return MPI_SUCCESS;
+}
+
+// whether p is host memory (pageable or pinned)
+bool host_memory(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return a.type == cudaMemoryTypeUnregistered || a.type == cudaMemoryTypeHost;
+}
+
+// One contiguous copy of a self-message, as a library's shared-memory path
+// would make it: host to host by memcpy (split over threads above 16 MiB,
+// as an optimised copy loop would run), anything touching device or managed
+// memory by cuda_copy.
+int copy_bytes(void *dst, const void *src, int64_t n) {
+  if (n <= 0)
+    return MPI_SUCCESS;
+  if (host_memory(src) && host_memory(dst)) {
+    constexpr int64_t kSplit = int64_t(16) << 20;
+    const int nt = n < kSplit ? 1 : int(std::min<int64_t>(8, n / kSplit));
+    if (nt == 1) {
+      std::memcpy(dst, src, size_t(n));
+      return MPI_SUCCESS;
+    }
+    std::vector<std::thread> ts;
+    const int64_t per = (n + nt - 1) / nt;
+    for (int i = 0; i < nt; ++i) {
+      const int64_t a = i * per, b = std::min(n, a + per);
+      if (a < b)
+        ts.emplace_back([=] {
+          std::memcpy(static_cast<char *>(dst) + a,
+                      static_cast<const char *>(src) + a, size_t(b - a));
+        });
+    }
+    for (auto &t : ts)
+      t.join();
+    return MPI_SUCCESS;
+  }
+  return cuda_copy(dst, src, size_t(n));
+}
+
 // byte span [lo, hi) touched by `count` objects of type t
 void span(const TypeRec &t, int64_t count, int64_t &lo, int64_t &hi) {
   if (count <= 0 || t.size == 0) {
@@ -307,8 +390,7 @@ int pack_any(const TypeRec &t, const void *buf, int64_t count,
   int64_t lo, hi;
   span(t, count, lo, hi);
   std::vector<char> stage(size_t(hi - lo));
-  if (cudaMemcpy(stage.data(), (const char *)buf + lo, hi - lo,
-                 cudaMemcpyDefault) != cudaSuccess)
+  if (cuda_copy(stage.data(), (const char *)buf + lo, size_t(hi - lo)))
     return MPI_ERR_OTHER;
   pack_host(t, stage.data() - lo, count, out.data());
   return MPI_SUCCESS;
@@ -326,10 +408,10 @@ int unpack_any(const TypeRec &t, const char *packed, int64_t count, void *buf) {
   span(t, count, lo, hi);
   std::vector<char> stage(size_t(hi - lo));
   char *dev = (char *)buf + lo;
-  if (cudaMemcpy(stage.data(), dev, hi - lo, cudaMemcpyDefault) != cudaSuccess)
+  if (cuda_copy(stage.data(), dev, size_t(hi - lo)))
     return MPI_ERR_OTHER;
   unpack_host(t, packed, count, stage.data() - lo);
-  if (cudaMemcpy(dev, stage.data(), hi - lo, cudaMemcpyDefault) != cudaSuccess)
+  if (cuda_copy(dev, stage.data(), size_t(hi - lo)))
     return MPI_ERR_OTHER;
   return MPI_SUCCESS;
 }
@@ -345,6 +427,7 @@ struct Message {
   std::vector<char> data; // host payload
   void *dev = nullptr;    // device payload, if any
   int64_t bytes = 0;
+  int source = 0; // sending rank
 };
 
 std::unordered_map<int64_t, std::vector<void *>> g_dev_pool;
@@ -395,6 +478,8 @@ struct Graph {
 std::unordered_map<MPI_Comm, Graph> g_graphs;
 MPI_Comm g_next_comm = 16;
 constexpr MPI_Comm kCollBit = 0x40000000;
+// tags of the library's own collectives (on collective contexts only)
+constexpr int kBarrierTag = 0x7ffffff0, kAlltoallvTag = 0x7ffffff1;
 
 bool valid_comm(MPI_Comm c) {
   c &= ~kCollBit;
@@ -421,14 +506,10 @@ int deliver(Req &r, const Message &m) {
     // contiguous receive: one copy, whatever memory either side is in
     char *dst = (char *)r.rbuf + t->lb;
     const void *src = m.dev ? m.dev : (const void *)m.data.data();
-    if (!m.dev && !is_device(r.rbuf))
-      std::memcpy(dst, src, n);
-    else if (cudaMemcpy(dst, src, n, cudaMemcpyDefault) != cudaSuccess)
-      e2 = MPI_ERR_OTHER;
+    e2 = copy_bytes(dst, src, n);
   } else if (m.dev) {
     std::vector<char> host(size_t(m.bytes));
-    if (cudaMemcpy(host.data(), m.dev, m.bytes, cudaMemcpyDefault) !=
-        cudaSuccess)
+    if (cuda_copy(host.data(), m.dev, size_t(m.bytes)))
       e2 = MPI_ERR_OTHER;
     else
       e2 = unpack_any(*t, host.data(), whole, r.rbuf);
@@ -437,12 +518,241 @@ int deliver(Req &r, const Message &m) {
   }
   if (e2 != MPI_SUCCESS)
     err = e2;
-  r.st.MPI_SOURCE = 0;
+  r.st.MPI_SOURCE = m.source;
   r.st.MPI_TAG = m.tag;
   r.st.MPI_ERROR = err;
   r.st.bytes_ = n;
   r.complete = true;
   return err;
+}
+
+// ---- ranks on one host -------------------------------------------------------
+
+int g_rank = 0, g_size = 1;
+double g_timeout_s = 60;
+std::string g_sock_path; // this rank's listening socket, removed at finalize
+
+struct Peer {
+  int fd = -1;
+  std::vector<char> in; // bytes read, not yet parsed into messages
+  size_t head = 0;      // first unparsed byte of `in`
+};
+std::vector<Peer> g_peers; // by rank; g_peers[g_rank] unused
+
+struct WireHeader {
+  uint32_t magic;
+  int32_t source, tag, comm;
+  int64_t bytes;
+};
+constexpr uint32_t kWireMagic = 0x314d504du;
+
+void arrive(Message &&m);
+
+// read what the sockets hold and hand every complete message to the matcher
+int progress_locked() {
+  if (g_size <= 1)
+    return MPI_SUCCESS;
+  static std::vector<char> tmp(size_t(1) << 20);
+  int err = MPI_SUCCESS;
+  for (int p = 0; p < g_size; ++p) {
+    Peer &pe = g_peers[p];
+    if (pe.fd < 0)
+      continue;
+    while (true) {
+      const ssize_t got = ::recv(pe.fd, tmp.data(), tmp.size(), 0);
+      if (got > 0) {
+        pe.in.insert(pe.in.end(), tmp.data(), tmp.data() + got);
+        continue;
+      }
+      if (got < 0 && errno == EINTR)
+        continue;
+      if (got < 0 && (errno == EAGAIN || errno == EWOULDBLOCK))
+        break;
+      // 0: the peer closed its end (it finalised); < 0: a real error
+      if (got < 0)
+        err = MPI_ERR_OTHER;
+      ::close(pe.fd);
+      pe.fd = -1;
+      break;
+    }
+    while (pe.in.size() - pe.head >= sizeof(WireHeader)) {
+      WireHeader h;
+      std::memcpy(&h, pe.in.data() + pe.head, sizeof(h));
+      if (h.magic != kWireMagic || h.bytes < 0) {
+        std::fprintf(stderr, "minimpi: corrupt message from rank %d\n", p);
+        return MPI_ERR_INTERN;
+      }
+      const size_t need = sizeof(h) + size_t(h.bytes);
+      if (pe.in.size() - pe.head < need)
+        break;
+      Message m{h.tag, MPI_Comm(h.comm), {}, nullptr, h.bytes, h.source};
+      const char *payload = pe.in.data() + pe.head + sizeof(h);
+      m.data.assign(payload, payload + h.bytes);
+      pe.head += need;
+      arrive(std::move(m));
+    }
+    if (pe.head > 0 && (pe.head == pe.in.size() || pe.head > (size_t(16) << 20))) {
+      pe.in.erase(pe.in.begin(), pe.in.begin() + ptrdiff_t(pe.head));
+      pe.head = 0;
+    }
+  }
+  return err;
+}
+
+// wait (up to ms milliseconds) until a socket has something to read, or
+// (want_write) until `write_fd` can take more
+void wait_io(int ms, int write_fd = -1) {
+  std::vector<pollfd> fds;
+  for (const Peer &pe : g_peers)
+    if (pe.fd >= 0)
+      fds.push_back({pe.fd, short(pe.fd == write_fd ? POLLIN | POLLOUT : POLLIN), 0});
+  if (!fds.empty())
+    ::poll(fds.data(), fds.size(), ms);
+}
+
+// write all of [p, p + n) to `fd`, reading incoming messages whenever the
+// socket is full, so that two ranks writing to each other both progress
+int write_all(int fd, const char *p, size_t n) {
+  const auto t0 = std::chrono::steady_clock::now();
+  while (n > 0) {
+    const ssize_t put = ::send(fd, p, n, MSG_NOSIGNAL);
+    if (put > 0) {
+      p += put;
+      n -= size_t(put);
+      continue;
+    }
+    if (put < 0 && errno == EINTR)
+      continue;
+    if (put < 0 && errno != EAGAIN && errno != EWOULDBLOCK)
+      return MPI_ERR_OTHER;
+    progress_locked();
+    wait_io(1, fd);
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0)
+            .count() > g_timeout_s)
+      return MPI_ERR_OTHER;
+  }
+  return MPI_SUCCESS;
+}
+
+// an eager send to another rank: the described bytes in MPI order
+int send_remote(const void *buf, int count, const TypeRec &t, int dest,
+                int tag, MPI_Comm comm) {
+  Peer &pe = g_peers[dest];
+  if (pe.fd < 0)
+    return MPI_ERR_OTHER;
+  std::vector<char> data;
+  int err = pack_any(t, buf, count, data);
+  if (err)
+    return err;
+  const WireHeader h{kWireMagic, g_rank, tag, int32_t(comm), int64_t(data.size())};
+  err = write_all(pe.fd, reinterpret_cast<const char *>(&h), sizeof(h));
+  if (!err)
+    err = write_all(pe.fd, data.data(), data.size());
+  return err;
+}
+
+// Join the world named by MINIMPI_SIZE / MINIMPI_RANK / MINIMPI_DIR: listen
+// on <dir>/r<rank>.sock, connect to every lower rank (sending our rank), and
+// accept every higher one.
+int world_init() {
+  const char *sz = std::getenv("MINIMPI_SIZE");
+  const char *rk = std::getenv("MINIMPI_RANK");
+  const char *dir = std::getenv("MINIMPI_DIR");
+  if (const char *t = std::getenv("MINIMPI_TIMEOUT_S"))
+    g_timeout_s = std::max(1.0, std::atof(t));
+  g_size = sz ? std::max(1, std::atoi(sz)) : 1;
+  g_rank = rk ? std::atoi(rk) : 0;
+  if (g_size <= 1) {
+    g_size = 1;
+    g_rank = 0;
+    return MPI_SUCCESS;
+  }
+  if (g_rank < 0 || g_rank >= g_size || !dir) {
+    std::fprintf(stderr, "minimpi: MINIMPI_SIZE=%d needs MINIMPI_RANK in range "
+                         "and MINIMPI_DIR\n", g_size);
+    return MPI_ERR_OTHER;
+  }
+  ::mkdir(dir, 0700);
+  g_peers.assign(size_t(g_size), Peer{});
+  auto path_of = [&](int r) { return std::string(dir) + "/r" + std::to_string(r) + ".sock"; };
+  const int lfd = ::socket(AF_UNIX, SOCK_STREAM, 0);
+  sockaddr_un a{};
+  a.sun_family = AF_UNIX;
+  g_sock_path = path_of(g_rank);
+  if (lfd < 0 || g_sock_path.size() >= sizeof(a.sun_path))
+    return MPI_ERR_OTHER;
+  std::strcpy(a.sun_path, g_sock_path.c_str());
+  ::unlink(a.sun_path);
+  if (::bind(lfd, reinterpret_cast<sockaddr *>(&a), sizeof(a)) != 0 ||
+      ::listen(lfd, g_size) != 0) {
+    ::close(lfd);
+    return MPI_ERR_OTHER;
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  auto late = [&] {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0)
+               .count() > g_timeout_s;
+  };
+  for (int p = 0; p < g_rank; ++p) { // connect to the lower ranks
+    sockaddr_un b{};
+    b.sun_family = AF_UNIX;
+    std::strcpy(b.sun_path, path_of(p).c_str());
+    int fd = -1;
+    while (true) {
+      fd = ::socket(AF_UNIX, SOCK_STREAM, 0);
+      if (fd >= 0 && ::connect(fd, reinterpret_cast<sockaddr *>(&b), sizeof(b)) == 0)
+        break;
+      if (fd >= 0)
+        ::close(fd);
+      fd = -1;
+      if (late()) {
+        ::close(lfd);
+        return MPI_ERR_OTHER;
+      }
+      ::usleep(2000);
+    }
+    const int32_t me = g_rank;
+    if (::send(fd, &me, sizeof(me), MSG_NOSIGNAL) != ssize_t(sizeof(me))) {
+      ::close(fd);
+      ::close(lfd);
+      return MPI_ERR_OTHER;
+    }
+    g_peers[p].fd = fd;
+  }
+  for (int k = g_rank + 1; k < g_size; ++k) { // accept the higher ranks
+    pollfd pf{lfd, POLLIN, 0};
+    while (::poll(&pf, 1, 10) == 0)
+      if (late()) {
+        ::close(lfd);
+        return MPI_ERR_OTHER;
+      }
+    const int fd = ::accept(lfd, nullptr, nullptr);
+    int32_t who = -1;
+    if (fd < 0 || ::recv(fd, &who, sizeof(who), MSG_WAITALL) != ssize_t(sizeof(who)) ||
+        who <= g_rank || who >= g_size || g_peers[who].fd >= 0) {
+      if (fd >= 0)
+        ::close(fd);
+      ::close(lfd);
+      return MPI_ERR_OTHER;
+    }
+    g_peers[who].fd = fd;
+  }
+  ::close(lfd);
+  for (Peer &pe : g_peers)
+    if (pe.fd >= 0)
+      ::fcntl(pe.fd, F_SETFL, ::fcntl(pe.fd, F_GETFL) | O_NONBLOCK);
+  return MPI_SUCCESS;
+}
+
+void world_finalize() {
+  for (Peer &pe : g_peers)
+    if (pe.fd >= 0) {
+      ::close(pe.fd);
+      pe.fd = -1;
+    }
+  if (!g_sock_path.empty())
+    ::unlink(g_sock_path.c_str());
+  g_sock_path.clear();
 }
 
 int do_send(const void *buf, int count, MPI_Datatype type, int dest, int tag,
@@ -451,18 +761,20 @@ int do_send(const void *buf, int count, MPI_Datatype type, int dest, int tag,
     return MPI_ERR_COMM;
   if (dest == MPI_PROC_NULL)
     return MPI_SUCCESS;
-  if (dest != 0)
+  if (dest < 0 || dest >= g_size)
     return MPI_ERR_RANK;
   if (count < 0)
     return MPI_ERR_COUNT;
   const TypeRec *t = get(type);
   if (!t)
     return MPI_ERR_TYPE;
+  if (dest != g_rank)
+    return send_remote(buf, count, *t, dest, tag, comm);
   // rendezvous: a matching receive is already posted and both sides are
   // contiguous, so the bytes go straight from buffer to buffer in one copy
   for (auto it = g_posted.begin(); it != g_posted.end(); ++it) {
     Req &r = g_reqs[*it];
-    if (r.comm != comm || !(r.peer == 0 || r.peer == MPI_ANY_SOURCE) ||
+    if (r.comm != comm || !(r.peer == g_rank || r.peer == MPI_ANY_SOURCE) ||
         !tag_match(r.tag, tag))
       continue;
     const TypeRec *rt = get(r.type);
@@ -478,48 +790,50 @@ int do_send(const void *buf, int count, MPI_Datatype type, int dest, int tag,
     }
     const char *src = (const char *)buf + t->lb;
     char *dst = (char *)r.rbuf + rt->lb;
-    if (n > 0) {
-      if (!is_device(src) && !is_device(dst))
-        std::memcpy(dst, src, size_t(n));
-      else if (cudaMemcpy(dst, src, size_t(n), cudaMemcpyDefault) != cudaSuccess)
-        err = MPI_ERR_OTHER;
-    }
-    r.st.MPI_SOURCE = 0;
+    if (int e = copy_bytes(dst, src, n))
+      err = e;
+    r.st.MPI_SOURCE = g_rank;
     r.st.MPI_TAG = tag;
     r.st.MPI_ERROR = err;
     r.st.bytes_ = n;
     r.complete = true;
     return MPI_SUCCESS;
   }
-  Message m{tag, comm, {}, nullptr, int64_t(count) * t->size};
+  Message m{tag, comm, {}, nullptr, int64_t(count) * t->size, g_rank};
   if (t->dense && m.bytes > 0 && is_device(buf)) {
     m.dev = dev_get(m.bytes);
-    if (!m.dev || cudaMemcpy(m.dev, (const char *)buf + t->lb, m.bytes,
-                             cudaMemcpyDefault) != cudaSuccess)
+    if (!m.dev || cuda_copy(m.dev, (const char *)buf + t->lb, size_t(m.bytes)))
       return MPI_ERR_OTHER;
   } else {
     int err = pack_any(*t, buf, count, m.data);
     if (err)
       return err;
   }
+  arrive(std::move(m));
+  return MPI_SUCCESS;
+}
+
+// a message from any rank: to the earliest matching posted receive, else
+// into the unexpected queue
+void arrive(Message &&m) {
   for (auto it = g_posted.begin(); it != g_posted.end(); ++it) {
     Req &r = g_reqs[*it];
-    if (r.comm == comm && (r.peer == 0 || r.peer == MPI_ANY_SOURCE) &&
-        tag_match(r.tag, tag)) {
+    if (r.comm == m.comm && (r.peer == m.source || r.peer == MPI_ANY_SOURCE) &&
+        tag_match(r.tag, m.tag)) {
       g_posted.erase(it);
       deliver(r, m);
       dev_put(m.dev, m.bytes);
-      return MPI_SUCCESS;
+      return;
     }
   }
   g_unexpected.push_back(std::move(m));
-  return MPI_SUCCESS;
 }
 
 // try to satisfy an active receive from the unexpected queue
 bool try_match(Req &r) {
   for (auto it = g_unexpected.begin(); it != g_unexpected.end(); ++it) {
-    if (it->comm == r.comm && tag_match(r.tag, it->tag)) {
+    if (it->comm == r.comm && tag_match(r.tag, it->tag) &&
+        (r.peer == MPI_ANY_SOURCE || r.peer == it->source)) {
       Message m = std::move(*it);
       g_unexpected.erase(it);
       deliver(r, m);
@@ -547,8 +861,9 @@ int start_req(int id) {
     r.st.MPI_TAG = MPI_ANY_TAG;
     return MPI_SUCCESS;
   }
-  if (r.peer != 0 && r.peer != MPI_ANY_SOURCE)
+  if (r.peer != MPI_ANY_SOURCE && (r.peer < 0 || r.peer >= g_size))
     return MPI_ERR_RANK;
+  progress_locked();
   if (!try_match(r))
     g_posted.push_back(id);
   return MPI_SUCCESS;
@@ -574,6 +889,17 @@ void finish_req(MPI_Request *request, MPI_Status *status) {
   }
 }
 
+// Test hook (minimpi_fail_nth): the n-th call of one entry point from then
+// on returns MPI_ERR_OTHER and does nothing, so the error paths of the
+// library's callers can be exercised on the host.  Caller holds g_mu.
+std::string g_fail_call;
+int g_fail_left = 0;
+bool injected_failure(const char *name) {
+  if (g_fail_left <= 0 || g_fail_call != name)
+    return false;
+  return --g_fail_left == 0;
+}
+
 int new_type(TypeRec &&t, MPI_Datatype *newtype) {
   if (!newtype)
     return MPI_ERR_ARG;
@@ -585,9 +911,25 @@ int new_type(TypeRec &&t, MPI_Datatype *newtype) {
 
 extern "C" {
 
+// Arms the failure of the n-th later call of `call` ("MPI_Send", "MPI_Recv",
+// "MPI_Irecv", "MPI_Send_init", "MPI_Start" or "MPI_Test"; calls the library
+// makes to itself count too); n <= 0 disarms it.  Not part of MPI: a test
+// hook of this stand-in library.
+int minimpi_fail_nth(const char *call, int n) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  g_fail_call = call ? call : "";
+  g_fail_left = n > 0 ? n : 0;
+  return MPI_SUCCESS;
+}
+
 int MPI_Init(int *, char ***) {
   std::lock_guard<std::recursive_mutex> l(g_mu);
   init_named();
+  if (!g_initialized) {
+    int err = world_init();
+    if (err)
+      return err;
+  }
   g_initialized = true;
   return MPI_SUCCESS;
 }
@@ -599,8 +941,12 @@ int MPI_Init_thread(int *argc, char ***argv, int required, int *provided) {
 }
 int MPI_Finalize(void) {
   std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (g_finalized)
+    return MPI_SUCCESS;
+  int err = g_size > 1 ? MPI_Barrier(MPI_COMM_WORLD) : MPI_SUCCESS;
+  world_finalize();
   g_finalized = true;
-  return MPI_SUCCESS;
+  return err;
 }
 int MPI_Initialized(int *flag) {
   *flag = g_initialized;
@@ -627,19 +973,49 @@ int MPI_Get_library_version(char *version, int *resultlen) {
   return MPI_SUCCESS;
 }
 int MPI_Comm_rank(MPI_Comm comm, int *rank) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
   if (!valid_comm(comm))
     return MPI_ERR_COMM;
-  *rank = 0;
+  *rank = comm == MPI_COMM_SELF ? 0 : g_rank;
   return MPI_SUCCESS;
 }
 int MPI_Comm_size(MPI_Comm comm, int *size) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
   if (!valid_comm(comm))
     return MPI_ERR_COMM;
-  *size = 1;
+  *size = comm == MPI_COMM_SELF ? 1 : g_size;
   return MPI_SUCCESS;
 }
+// Every rank sends an empty message to every other rank on the world's
+// collective context and waits for all of theirs.
 int MPI_Barrier(MPI_Comm comm) {
-  return valid_comm(comm) ? MPI_SUCCESS : MPI_ERR_COMM;
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!valid_comm(comm))
+    return MPI_ERR_COMM;
+  if (g_size <= 1 || comm == MPI_COMM_SELF)
+    return MPI_SUCCESS;
+  const MPI_Comm cc = MPI_COMM_WORLD | kCollBit;
+  std::vector<MPI_Request> reqs;
+  char none = 0;
+  int err = MPI_SUCCESS;
+  for (int p = 0; p < g_size && !err; ++p) {
+    if (p == g_rank)
+      continue;
+    MPI_Request r;
+    err = MPI_Irecv(&none, 0, MPI_BYTE, p, kBarrierTag, cc, &r);
+    if (!err)
+      reqs.push_back(r);
+  }
+  for (int p = 0; p < g_size && !err; ++p) {
+    if (p == g_rank)
+      continue;
+    MPI_Request r;
+    err = MPI_Isend(&none, 0, MPI_BYTE, p, kBarrierTag, cc, &r);
+    if (!err)
+      reqs.push_back(r);
+  }
+  const int werr = MPI_Waitall(int(reqs.size()), reqs.data(), MPI_STATUSES_IGNORE);
+  return err ? err : werr;
 }
 int MPI_Error_string(int errorcode, char *string, int *resultlen) {
   std::snprintf(string, 64, "MPI error %d", errorcode);
@@ -1048,8 +1424,7 @@ int MPI_Pack(const void *inbuf, int incount, MPI_Datatype datatype,
     return err;
   char *dst = (char *)outbuf + *position;
   if (is_device(outbuf)) {
-    if (need && cudaMemcpy(dst, packed.data(), need, cudaMemcpyDefault) !=
-                    cudaSuccess)
+    if (need && cuda_copy(dst, packed.data(), size_t(need)))
       return MPI_ERR_OTHER;
   } else if (need) {
     std::memcpy(dst, packed.data(), need);
@@ -1075,8 +1450,7 @@ int MPI_Unpack(const void *inbuf, int insize, int *position, void *outbuf,
   const char *src = (const char *)inbuf + *position;
   if (need) {
     if (is_device(inbuf)) {
-      if (cudaMemcpy(packed.data(), src, need, cudaMemcpyDefault) !=
-          cudaSuccess)
+      if (cuda_copy(packed.data(), src, size_t(need)))
         return MPI_ERR_OTHER;
     } else {
       std::memcpy(packed.data(), src, need);
@@ -1104,12 +1478,16 @@ int MPI_Pack_size(int incount, MPI_Datatype datatype, MPI_Comm comm,
 int MPI_Send(const void *buf, int count, MPI_Datatype datatype, int dest,
              int tag, MPI_Comm comm) {
   std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (injected_failure("MPI_Send"))
+    return MPI_ERR_OTHER;
   return do_send(buf, count, datatype, dest, tag, comm);
 }
 
 int MPI_Recv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
              MPI_Comm comm, MPI_Status *status) {
   std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (injected_failure("MPI_Recv"))
+    return MPI_ERR_OTHER;
   MPI_Request req;
   int err = MPI_Irecv(buf, count, datatype, source, tag, comm, &req);
   if (err)
@@ -1133,6 +1511,8 @@ int MPI_Isend(const void *buf, int count, MPI_Datatype datatype, int dest,
 int MPI_Irecv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
               MPI_Comm comm, MPI_Request *request) {
   std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (injected_failure("MPI_Irecv"))
+    return MPI_ERR_OTHER;
   int err = MPI_Recv_init(buf, count, datatype, source, tag, comm, request);
   if (err)
     return err;
@@ -1143,6 +1523,8 @@ int MPI_Irecv(void *buf, int count, MPI_Datatype datatype, int source, int tag,
 int MPI_Send_init(const void *buf, int count, MPI_Datatype datatype, int dest,
                   int tag, MPI_Comm comm, MPI_Request *request) {
   std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (injected_failure("MPI_Send_init"))
+    return MPI_ERR_OTHER;
   if (!valid_comm(comm))
     return MPI_ERR_COMM;
   if (!get(datatype))
@@ -1182,6 +1564,8 @@ int MPI_Recv_init(void *buf, int count, MPI_Datatype datatype, int source,
 
 int MPI_Start(MPI_Request *request) {
   std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (injected_failure("MPI_Start"))
+    return MPI_ERR_OTHER;
   if (!request || !g_reqs.count(*request))
     return MPI_ERR_REQUEST;
   Req &r = g_reqs[*request];
@@ -1192,6 +1576,9 @@ int MPI_Start(MPI_Request *request) {
 
 int MPI_Test(MPI_Request *request, int *flag, MPI_Status *status) {
   std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (injected_failure("MPI_Test"))
+    return MPI_ERR_OTHER;
+  progress_locked();
   if (!request)
     return MPI_ERR_REQUEST;
   if (*request == MPI_REQUEST_NULL) {
@@ -1220,14 +1607,28 @@ int MPI_Wait(MPI_Request *request, MPI_Status *status) {
   int err = MPI_Test(request, &flag, status);
   if (err)
     return err;
-  if (!flag) {
+  if (flag)
+    return MPI_SUCCESS;
+  if (g_size <= 1) {
     // one rank, one thread: no send can arrive while we block
     std::fprintf(stderr,
                  "minimpi: MPI_Wait on a receive with no matching send "
                  "(would deadlock at world size 1)\n");
     return MPI_ERR_OTHER;
   }
-  return MPI_SUCCESS;
+  const auto t0 = std::chrono::steady_clock::now();
+  while (true) {
+    wait_io(1);
+    err = MPI_Test(request, &flag, status);
+    if (err || flag)
+      return err;
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0)
+            .count() > g_timeout_s) {
+      std::fprintf(stderr, "minimpi: rank %d gave up waiting after %.0f s\n",
+                   g_rank, g_timeout_s);
+      return MPI_ERR_OTHER;
+    }
+  }
 }
 
 int MPI_Waitall(int count, MPI_Request reqs[], MPI_Status stats[]) {
@@ -1249,7 +1650,7 @@ int MPI_Dist_graph_create_adjacent(MPI_Comm comm_old, int indegree,
                                    const int destweights[], MPI_Info info,
                                    int reorder, MPI_Comm *comm_dist_graph) {
   (void)info;
-  (void)reorder; // one rank: nothing to reorder
+  (void)reorder; // ranks keep their numbers
   std::lock_guard<std::recursive_mutex> l(g_mu);
   if (!valid_comm(comm_old) || (comm_old & kCollBit))
     return MPI_ERR_COMM;
@@ -1259,17 +1660,17 @@ int MPI_Dist_graph_create_adjacent(MPI_Comm comm_old, int indegree,
   Graph g;
   g.weighted = sourceweights != MPI_UNWEIGHTED && destweights != MPI_UNWEIGHTED;
   for (int i = 0; i < indegree; ++i) {
-    if (sources[i] != 0)
+    if (sources[i] < 0 || sources[i] >= g_size)
       return MPI_ERR_RANK;
-    g.sources.push_back(0);
+    g.sources.push_back(sources[i]);
     g.sweights.push_back(g.weighted && sourceweights != MPI_WEIGHTS_EMPTY
                              ? sourceweights[i]
                              : 1);
   }
   for (int i = 0; i < outdegree; ++i) {
-    if (destinations[i] != 0)
+    if (destinations[i] < 0 || destinations[i] >= g_size)
       return MPI_ERR_RANK;
-    g.dests.push_back(0);
+    g.dests.push_back(destinations[i]);
     g.dweights.push_back(g.weighted && destweights != MPI_WEIGHTS_EMPTY
                              ? destweights[i]
                              : 1);
@@ -1409,6 +1810,43 @@ int MPI_Neighbor_alltoallw(const void *sendbuf, const int sendcounts[],
         *n = recvcounts[j];
         *t = recvtypes[j];
       });
+}
+
+// Every rank's block to every rank: one receive per source and one send per
+// destination on the communicator's collective context, then wait for all.
+int MPI_Alltoallv(const void *sendbuf, const int sendcounts[],
+                  const int sdispls[], MPI_Datatype sendtype, void *recvbuf,
+                  const int recvcounts[], const int rdispls[],
+                  MPI_Datatype recvtype, MPI_Comm comm) {
+  std::lock_guard<std::recursive_mutex> l(g_mu);
+  if (!valid_comm(comm) || (comm & kCollBit))
+    return MPI_ERR_COMM;
+  const TypeRec *st = get(sendtype), *rt = get(recvtype);
+  if (!st || !rt)
+    return MPI_ERR_TYPE;
+  const int n = comm == MPI_COMM_SELF ? 1 : g_size;
+  const int me = comm == MPI_COMM_SELF ? 0 : g_rank;
+  const MPI_Comm cc = comm | kCollBit;
+  std::vector<MPI_Request> reqs;
+  int err = MPI_SUCCESS;
+  for (int i = 0; i < n && !err; ++i) {
+    MPI_Request r;
+    err = MPI_Irecv((char *)recvbuf + int64_t(rdispls[i]) * rt->extent(),
+                    recvcounts[i], recvtype, comm == MPI_COMM_SELF ? me : i,
+                    kAlltoallvTag, cc, &r);
+    if (!err)
+      reqs.push_back(r);
+  }
+  for (int j = 0; j < n && !err; ++j) {
+    MPI_Request r;
+    err = MPI_Isend((const char *)sendbuf + int64_t(sdispls[j]) * st->extent(),
+                    sendcounts[j], sendtype, comm == MPI_COMM_SELF ? me : j,
+                    kAlltoallvTag, cc, &r);
+    if (!err)
+      reqs.push_back(r);
+  }
+  const int werr = MPI_Waitall(int(reqs.size()), reqs.data(), MPI_STATUSES_IGNORE);
+  return err ? err : werr;
 }
 
 int MPI_Request_free(MPI_Request *request) {

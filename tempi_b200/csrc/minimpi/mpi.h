@@ -130,6 +130,9 @@ int MPI_Get_library_version(char *version, int *resultlen);
 int MPI_Comm_rank(MPI_Comm comm, int *rank);
 int MPI_Comm_size(MPI_Comm comm, int *size);
 int MPI_Barrier(MPI_Comm comm);
+int MPI_Alltoallv(const void *sendbuf, const int sendcounts[], const int sdispls[],
+                  MPI_Datatype sendtype, void *recvbuf, const int recvcounts[],
+                  const int rdispls[], MPI_Datatype recvtype, MPI_Comm comm);
 int MPI_Error_string(int errorcode, char *string, int *resultlen);
 
 /* datatypes */

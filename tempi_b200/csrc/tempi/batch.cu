@@ -529,7 +529,7 @@ static int upload(const std::vector<Rec> &recs, Rec **dev) {
   if (!*dev)
     e = cudaMalloc(dev, bytes);
   if (e == cudaSuccess)
-    e = cudaMemcpy(*dev, recs.data(), bytes, cudaMemcpyHostToDevice);
+    e = copy_complete(*dev, recs.data(), bytes);
   if (e != cudaSuccess)
     return cuda_error(e, "batch table upload");
   return TEMPI_OK;

@@ -152,8 +152,8 @@ int predict(const float f[TEMPI_MLP_IN], float mean[TEMPI_MLP_OUT],
   if (!m.dev_params) {
     e = cudaMalloc(&m.dev_params, m.params.size() * sizeof(float));
     if (e == cudaSuccess)
-      e = cudaMemcpy(m.dev_params, m.params.data(),
-                     m.params.size() * sizeof(float), cudaMemcpyHostToDevice);
+      e = copy_complete(m.dev_params, m.params.data(),
+                        m.params.size() * sizeof(float));
     void *h = nullptr, *d = nullptr;
     if (e == cudaSuccess)
       e = cudaHostAlloc(&h, io_floats * sizeof(float), cudaHostAllocMapped);

@@ -34,6 +34,12 @@ int log_level();
 int set_error(int code, const char *fmt, ...);
 int cuda_error(cudaError_t e, const char *what);
 
+// Copy n bytes and return only once they have landed.  A plain cudaMemcpy
+// from pageable host memory (or between device buffers) can return before
+// the copy is done, and work the caller then issues on a non-blocking stream
+// is not ordered after it; this runs the copy on a private stream and waits.
+cudaError_t copy_complete(void *dst, const void *src, size_t n);
+
 // ---- counters (reference include/counters.hpp:14-115) ----------------------
 struct Counters {
   std::atomic<int64_t> kernel_launches{0};
@@ -46,11 +52,15 @@ struct Counters {
       recv_lib{0};
   std::atomic<int64_t> isend_managed{0}, irecv_managed{0};
   std::atomic<int64_t> dispatch_hit{0}, dispatch_miss{0};
-  std::atomic<int64_t> slab_hits{0}, slab_misses{0}, slab_bytes{0};
+  std::atomic<int64_t> slab_hits{0}, slab_misses{0};
+  // bytes held from CUDA (live + cached), handed out, kept for reuse
+  std::atomic<int64_t> slab_bytes{0}, slab_live_bytes{0}, slab_cached_bytes{0};
   std::atomic<int64_t> cached_types{0};
   std::atomic<int64_t> host_link_copies{0};
   std::atomic<int64_t> send_contig_staged{0}, recv_contig_staged{0};
   std::atomic<int64_t> neighbor_fused{0}, neighbor_isir{0}, neighbor_lib{0};
+  std::atomic<int64_t> alltoallv_staged{0}, alltoallv_remote_first{0},
+      alltoallv_isir_staged{0}, alltoallv_isir_remote_staged{0}, alltoallv_lib{0};
 };
 Counters &counters();
 

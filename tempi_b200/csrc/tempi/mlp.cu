@@ -349,8 +349,7 @@ extern "C" int tempi_mlp_init(float *params, int members, uint64_t seed) {
     fill(oW2, kHid, kHid);
     fill(oW3, kOut, kHid);
   }
-  cudaError_t e = cudaMemcpy(params, h.data(), h.size() * sizeof(float),
-                             cudaMemcpyDefault);
+  cudaError_t e = copy_complete(params, h.data(), h.size() * sizeof(float));
   return e == cudaSuccess ? TEMPI_OK : cuda_error(e, "mlp init upload");
 }
 

@@ -348,6 +348,26 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar,
   return true;
 }
 
+// The give-up path of a staged CTA, run by one thread: report the failure,
+// then wait once more (bounded again) on every stage that still has copies
+// counted -- the stage whose wait ran out included -- so that a copy that
+// was only slow lands before the CTA exits.  A copy still in flight after
+// this second bound (about two seconds in all) would write into the shared
+// memory of an exited CTA; nothing in this library issues such a copy (every
+// bulk copy reads device memory proper), so that case is a GPU fault, not a
+// path this code expects.
+__device__ __forceinline__ void staged_drain(const StagedCtl &ctl,
+                                             uint64_t *bar, uint32_t c,
+                                             uint32_t it, uint32_t nchunks) {
+  staged_give_up(ctl);
+  for (int k = 0; k < kStagedStages; ++k) {
+    const uint32_t ck = c + uint32_t(k) * gridDim.x;
+    if (ck < nchunks)
+      mbar_wait_bounded(&bar[(it + k) % kStagedStages],
+                        ((it + k) / kStagedStages) & 1);
+  }
+}
+
 template <int W, int ND>
 __global__ void __launch_bounds__(kStagedThreads)
     k_unpack_staged(char *__restrict__ strided,
@@ -384,16 +404,8 @@ __global__ void __launch_bounds__(kStagedThreads)
       gave_up = 1;
     __syncthreads();
     if (gave_up) {
-      if (threadIdx.x == 0) {
-        staged_give_up(ctl);
-        // the copies still counted on the other stages, bounded again
-        for (int k = 1; k < kStagedStages; ++k) {
-          const uint32_t ck = c + uint32_t(k) * gridDim.x;
-          if (ck < nchunks)
-            mbar_wait_bounded(&bar[(it + k) % kStagedStages],
-                              ((it + k) / kStagedStages) & 1);
-        }
-      }
+      if (threadIdx.x == 0)
+        staged_drain(ctl, bar, c, it, nchunks);
       return;
     }
     const uint32_t words = chunk_bytes(c) / W;
@@ -486,15 +498,8 @@ __global__ void __launch_bounds__(kStagedThreads)
       gave_up = 1;
     __syncthreads();
     if (gave_up) {
-      if (threadIdx.x == 0) {
-        staged_give_up(ctl);
-        for (int k = 1; k < kStagedStages; ++k) {
-          const uint32_t ck = c + uint32_t(k) * gridDim.x;
-          if (ck < nchunks)
-            mbar_wait_bounded(&bar[(it + k) % kStagedStages],
-                              ((it + k) / kStagedStages) & 1);
-        }
-      }
+      if (threadIdx.x == 0)
+        staged_drain(ctl, bar, c, it, nchunks);
       return;
     }
     const uint32_t words = chunk_bytes(c) / 16;
@@ -684,17 +689,31 @@ static const char *kernel_name(int kernel, uint32_t width, bool unpack) {
   return names[kernel - 1][unpack][width];
 }
 
+// SM count of the current device, cached per device index (a process may
+// drive GPUs with different SM counts)
 int num_sms() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
-            cudaSuccess) {
-      cudaGetLastError();
-      sms = 148;
-    }
+  constexpr int kDevs = 64;
+  static std::atomic<int> cache[kDevs];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    dev = -1;
   }
+  if (dev >= 0 && dev < kDevs) {
+    const int c = cache[dev].load(std::memory_order_relaxed);
+    if (c > 0)
+      return c;
+  }
+  int sms = 0;
+  if (dev < 0 ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+          cudaSuccess ||
+      sms <= 0) {
+    cudaGetLastError();
+    return 148;
+  }
+  if (dev < kDevs)
+    cache[dev].store(sms, std::memory_order_relaxed);
   return sms;
 }
 

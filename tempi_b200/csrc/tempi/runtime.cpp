@@ -54,6 +54,24 @@ void read_env() {
     e.host_link_dma = std::string(s) != "kernel";
   if (const char *s = std::getenv("TEMPI_TEST_STAGED_SHORTFALL"))
     e.staged_shortfall = std::max(0, std::min(4096, std::atoi(s))) & ~15;
+  if (has("TEMPI_ALLTOALLV_REMOTE_FIRST"))
+    e.alltoallv = Alltoallv::REMOTE_FIRST;
+  if (has("TEMPI_ALLTOALLV_STAGED"))
+    e.alltoallv = Alltoallv::STAGED;
+  if (has("TEMPI_ALLTOALLV_ISIR_STAGED"))
+    e.alltoallv = Alltoallv::ISIR_STAGED;
+  if (has("TEMPI_ALLTOALLV_ISIR_REMOTE_STAGED"))
+    e.alltoallv = Alltoallv::ISIR_REMOTE_STAGED;
+  if (has("TEMPI_NO_ALLTOALLV"))
+    e.alltoallv = Alltoallv::NONE;
+  if (const char *s = std::getenv("TEMPI_RANKS_PER_NODE"))
+    e.ranks_per_node = std::max(0, std::atoi(s));
+  if (const char *s = std::getenv("TEMPI_SLAB_CACHE_MB"))
+    e.slab_cache_mb = std::max(0L, std::atol(s));
+  // test-only: the n-th slab allocation from here on fails
+  slab_test_fail_after(std::getenv("TEMPI_TEST_FAIL_SLAB")
+                           ? std::atoll(std::getenv("TEMPI_TEST_FAIL_SLAB"))
+                           : 0);
   if (const char *cd = std::getenv("TEMPI_CACHE_DIR")) {
     e.cache_dir = cd;
   } else if (const char *x = std::getenv("XDG_CACHE_HOME")) {
@@ -136,14 +154,27 @@ PtrInfo classify(const void *p) {
 }
 
 // ---- slab allocators --------------------------------------------------------
+//
+// Intermediate packed buffers of the senders (reference allocator_slab.hpp:
+// power-of-two slabs kept for reuse).  Requests up to 64 MiB round up to a
+// power of two and come back through per-class free lists; larger ones round
+// up to a multiple of 2 MiB, so a 1 GiB + 1 B message takes 1 GiB + 2 MiB,
+// not 2 GiB.  Freed blocks are kept for reuse only while the bytes kept stay
+// within TEMPI_SLAB_CACHE_MB (default 4 GiB) per memory space; beyond that
+// a freed block goes straight back to CUDA.
 
 namespace {
+constexpr int kMaxClass = 26; // 64 MiB
+constexpr size_t kLargeGrain = size_t(2) << 20;
 struct Slab {
-  std::vector<void *> free_[64];
-  std::unordered_map<void *, int> cls;
+  std::vector<void *> free_[kMaxClass + 1];
+  std::vector<std::pair<size_t, void *>> large; // cached blocks above 64 MiB
+  std::unordered_map<void *, size_t> size_of;   // every block this space owns
+  size_t cached = 0, live = 0;
 };
 std::mutex g_slab_mu;
 Slab g_slabs[2];
+std::atomic<int64_t> g_fail_countdown{0};
 
 int size_class(size_t bytes) {
   int c = 8; // 256 B minimum
@@ -151,20 +182,70 @@ int size_class(size_t bytes) {
     ++c;
   return c;
 }
+
+size_t block_size(size_t bytes) {
+  const int c = size_class(bytes);
+  if (c <= kMaxClass)
+    return size_t(1) << c;
+  return (bytes + kLargeGrain - 1) / kLargeGrain * kLargeGrain;
+}
+
+void release_block(Space s, void *p) {
+  cudaError_t e = s == Space::DEVICE ? cudaFree(p) : cudaFreeHost(p);
+  if (e != cudaSuccess)
+    cuda_error(e, "slab release");
+}
+
+void update_gauges() {
+  counters().slab_live_bytes =
+      int64_t(g_slabs[0].live + g_slabs[1].live);
+  counters().slab_cached_bytes =
+      int64_t(g_slabs[0].cached + g_slabs[1].cached);
+}
 } // namespace
 
+void slab_test_fail_after(int64_t n) { g_fail_countdown = n > 0 ? n : 0; }
+
 void *slab_alloc(Space s, size_t bytes) {
-  const int c = size_class(bytes);
+  // the test-only failure countdown (TEMPI_TEST_FAIL_SLAB): the n-th
+  // allocation from when the knob was read fails as if CUDA had refused it
+  int64_t left = g_fail_countdown.load();
+  while (left > 0 && !g_fail_countdown.compare_exchange_weak(left, left - 1)) {
+  }
+  if (left == 1) {
+    set_error(TEMPI_ERR_NO_MEM, "slab allocation failed (injected by TEMPI_TEST_FAIL_SLAB)");
+    return nullptr;
+  }
+  const size_t n = block_size(bytes);
   std::lock_guard<std::mutex> l(g_slab_mu);
   Slab &sl = g_slabs[int(s)];
-  if (!sl.free_[c].empty()) {
-    void *p = sl.free_[c].back();
-    sl.free_[c].pop_back();
+  void *p = nullptr;
+  if (n <= (size_t(1) << kMaxClass)) {
+    auto &fl = sl.free_[size_class(n)];
+    if (!fl.empty()) {
+      p = fl.back();
+      fl.pop_back();
+    }
+  } else {
+    // the smallest cached large block that fits with at most 1/4 to spare
+    size_t best = 0;
+    for (size_t i = 0; i < sl.large.size(); ++i)
+      if (sl.large[i].first >= n && sl.large[i].first <= n + n / 4 &&
+          (!p || sl.large[i].first < sl.large[best].first)) {
+        best = i;
+        p = sl.large[i].second;
+      }
+    if (p)
+      sl.large.erase(sl.large.begin() + best);
+  }
+  if (p) {
+    const size_t have = sl.size_of[p];
+    sl.cached -= have;
+    sl.live += have;
     counters().slab_hits++;
+    update_gauges();
     return p;
   }
-  void *p = nullptr;
-  const size_t n = size_t(1) << c;
   cudaError_t e = s == Space::DEVICE
                       ? cudaMalloc(&p, n)
                       : cudaHostAlloc(&p, n, cudaHostAllocMapped |
@@ -173,9 +254,11 @@ void *slab_alloc(Space s, size_t bytes) {
     cuda_error(e, "slab allocation");
     return nullptr;
   }
-  sl.cls[p] = c;
+  sl.size_of[p] = n;
+  sl.live += n;
   counters().slab_misses++;
   counters().slab_bytes += int64_t(n);
+  update_gauges();
   return p;
 }
 
@@ -184,27 +267,41 @@ void slab_free(Space s, void *p) {
     return;
   std::lock_guard<std::mutex> l(g_slab_mu);
   Slab &sl = g_slabs[int(s)];
-  auto it = sl.cls.find(p);
-  if (it == sl.cls.end()) {
+  auto it = sl.size_of.find(p);
+  if (it == sl.size_of.end()) {
     LOG_ERROR("slab_free of a pointer this allocator does not own");
     return;
   }
-  sl.free_[it->second].push_back(p);
+  const size_t n = it->second;
+  sl.live -= n;
+  const size_t cap = size_t(env().slab_cache_mb) << 20;
+  if (sl.cached + n > cap) { // over the cap: back to CUDA
+    sl.size_of.erase(it);
+    counters().slab_bytes -= int64_t(n);
+    release_block(s, p);
+  } else {
+    sl.cached += n;
+    if (n <= (size_t(1) << kMaxClass))
+      sl.free_[size_class(n)].push_back(p);
+    else
+      sl.large.push_back({n, p});
+  }
+  update_gauges();
 }
 
 void slab_release_all() {
   std::lock_guard<std::mutex> l(g_slab_mu);
   for (int s = 0; s < 2; ++s) {
-    for (auto &kv : g_slabs[s].cls) {
-      if (s == int(Space::DEVICE))
-        cudaFree(kv.first);
-      else
-        cudaFreeHost(kv.first);
-    }
-    g_slabs[s].cls.clear();
+    for (auto &kv : g_slabs[s].size_of)
+      release_block(Space(s), kv.first);
+    g_slabs[s].size_of.clear();
     for (auto &f : g_slabs[s].free_)
       f.clear();
+    g_slabs[s].large.clear();
+    g_slabs[s].cached = g_slabs[s].live = 0;
   }
+  counters().slab_bytes = 0;
+  update_gauges();
 }
 
 // ---- events ---------------------------------------------------------------

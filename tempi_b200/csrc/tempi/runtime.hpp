@@ -16,6 +16,8 @@ namespace tempi {
 enum class Method { AUTO = 0, DEVICE = 1, ONESHOT = 2, STAGED = 3 };
 enum class Contiguous { NONE, AUTO, STAGED };
 enum class Dispatch { LEARNED, TABLE, EXHAUSTIVE, HEURISTIC };
+// the reference's MPI_Alltoallv methods (src/internal/alltoallv_impl.cpp)
+enum class Alltoallv { AUTO, STAGED, REMOTE_FIRST, ISIR_STAGED, ISIR_REMOTE_STAGED, NONE };
 
 struct Env {
   bool disable = false;      // TEMPI_DISABLE
@@ -34,6 +36,17 @@ struct Env {
   // bounded wait runs out (about a second) and the give-up path reports a
   // timeout.  For tests of that path only; 0 (the default) in normal use.
   int staged_shortfall = 0;
+  // TEMPI_SLAB_CACHE_MB: bytes of freed slabs kept for reuse, per memory
+  // space; freed slabs beyond it go back to CUDA.  Large enough by default
+  // that a loop of 1 GiB self-sends (a send slab and a receive slab) reuses
+  // its slabs instead of pinning (or allocating) gigabytes for every message.
+  long slab_cache_mb = 4096;
+  // TEMPI_ALLTOALLV_{STAGED,REMOTE_FIRST,ISIR_STAGED,ISIR_REMOTE_STAGED},
+  // TEMPI_NO_ALLTOALLV (reference src/internal/env.cpp:35-49)
+  Alltoallv alltoallv = Alltoallv::AUTO;
+  // TEMPI_RANKS_PER_NODE=k: ranks r and s share a node when r/k == s/k
+  // (0, the default: every rank of the job shares one node)
+  int ranks_per_node = 0;
 };
 const Env &env();
 void read_env(); // re-read the environment (MPI_Init does this)
@@ -79,12 +92,18 @@ struct PtrInfo {
 PtrInfo classify(const void *p);
 
 // ---- slab allocators (reference include/allocator_slab.hpp) ---------------
-// Power-of-two size classes with O(1) free lists.  Device slabs come from
+// Power-of-two size classes up to 64 MiB with O(1) free lists, blocks
+// rounded to 2 MiB above that; freed blocks are kept while the cached bytes
+// stay within TEMPI_SLAB_CACHE_MB per space.  Device slabs come from
 // cudaMalloc; host slabs from cudaHostAlloc(Mapped|Portable), so kernels can
-// write them directly (the ONE_SHOT path).
+// write them directly (the ONE_SHOT path).  slab_alloc returns null when the
+// allocation fails (tempi_last_error says why).
 enum class Space { DEVICE, HOST_MAPPED };
 void *slab_alloc(Space s, size_t bytes);
 void slab_free(Space s, void *p);
+// test hook behind TEMPI_TEST_FAIL_SLAB: the n-th slab_alloc from now fails
+// (0: none)
+void slab_test_fail_after(int64_t n);
 void slab_release_all();
 
 // ---- copy-engine path between pinned host buffers -------------------------

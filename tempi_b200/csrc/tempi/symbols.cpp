@@ -81,6 +81,7 @@ bool resolve_symbols() {
     LOAD(Dist_graph_neighbors_count);
     LOAD(Dist_graph_neighbors);
     LOAD(Neighbor_alltoallw);
+    LOAD(Alltoallv);
 #undef LOAD
     ok = r;
   });

@@ -49,6 +49,8 @@ struct LibMPI {
   int (*Neighbor_alltoallw)(const void *, const int[], const MPI_Aint[],
                             const MPI_Datatype[], void *, const int[],
                             const MPI_Aint[], const MPI_Datatype[], MPI_Comm);
+  int (*Alltoallv)(const void *, const int[], const int[], MPI_Datatype,
+                   void *, const int[], const int[], MPI_Datatype, MPI_Comm);
 };
 
 // Resolve the table once; returns false (and logs) if any symbol is missing.

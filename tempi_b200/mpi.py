@@ -252,6 +252,36 @@ def Neighbor_alltoallw(sendbuf: int, sendcounts, sdispls, sendtypes, recvbuf: in
         _ints(recvcounts), _aints(rdispls), _ints(recvtypes), comm)
 
 
+def Alltoallv(sendbuf: int, sendcounts, sdispls, sendtype: int, recvbuf: int, recvcounts,
+              rdispls, recvtype: int, comm: int = None, library: bool = False) -> int:
+    """MPI_Alltoallv; displacements in extents of the types.  ``library=True``
+    calls the underlying MPI directly."""
+    lib = _lib.minimpi() if library else _lib.tempi()
+    return lib.MPI_Alltoallv(sendbuf, _ints(sendcounts), _ints(sdispls), sendtype, recvbuf,
+                             _ints(recvcounts), _ints(rdispls), recvtype,
+                             COMM_WORLD if comm is None else comm)
+
+
+def Comm_rank(comm: int = None) -> int:
+    out = ctypes.c_int(0)
+    err = _lib.minimpi().MPI_Comm_rank(COMM_WORLD if comm is None else comm, ctypes.byref(out))
+    if err:
+        raise RuntimeError(f"MPI_Comm_rank failed with {err}")
+    return out.value
+
+
+def Comm_size(comm: int = None) -> int:
+    out = ctypes.c_int(0)
+    err = _lib.minimpi().MPI_Comm_size(COMM_WORLD if comm is None else comm, ctypes.byref(out))
+    if err:
+        raise RuntimeError(f"MPI_Comm_size failed with {err}")
+    return out.value
+
+
+def Barrier(comm: int = None) -> int:
+    return _lib.minimpi().MPI_Barrier(COMM_WORLD if comm is None else comm)
+
+
 def describe(t: int):
     """TEMPI's canonical strided block for a type (tempi_describe)."""
     d = _lib.Desc()

@@ -94,10 +94,12 @@ def test_launch_list_summary(tmp_path):
     add("tempi::k_mlp_predict(const float *, const float *, int, float *)", 9000)
     for i, (label, direction) in enumerate(bench.launch_list_order()):
         add("(anonymous namespace)::read_all(const uint4 *, unsigned long, unsigned int *)", 80000)
-        ns = {"empty": 1900, "gather": 3500}.get(label, 3000 + 10 * i)
-        name = {"empty": "(anonymous namespace)::k_bench_empty()",
-                "gather": "(anonymous namespace)::k_bench_gather(const char *, long long, int, "
-                          "unsigned int *)"}.get(
+        ns = {"empty": 1900, "gather": 3500, "gather_big": 1900 + 6554}.get(
+            label, 3000 + 10 * i)
+        gname = ("(anonymous namespace)::k_bench_gather(const char *, long long, int, "
+                 "unsigned int *)")
+        name = {"empty": "(anonymous namespace)::k_bench_empty()", "gather": gname,
+                "gather_big": gname}.get(
             label, "void tempi::k_words<4, 1, 0>(char *, char *, tempi::Geometry)")
         add(name, ns)
     csv = tmp_path / "launches.csv"
@@ -106,6 +108,7 @@ def test_launch_list_summary(tmp_path):
     bench.summarize_launches(str(csv), str(out))
     txt = out.read_text().splitlines()
     assert "empty kernel 1.90 us" in txt[0] and "gather 3.50 us" in txt[0]
+    assert "scattered line 25.00 ps" in txt[0]
     got = dict(((l.split()[0], l.split()[1]), float(l.split()[2])) for l in txt[1:])
     assert len(got) == 2 * len(bench.sweep_points())
     order = bench.launch_list_order()
