@@ -9,6 +9,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <chrono>
 #include <cstdint>
 
 #include "tempi_b200.h"
@@ -91,6 +93,59 @@ int tempi_bench_gather(const void *base, long long stride, int rows, void *out,
   k_bench_gather<<<(rows + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const char *>(base), stride, rows, static_cast<uint32_t *>(out));
   return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// Host wall-clock cost per call of the pieces of a synchronous MPI_Pack:
+// us_out[0] MPI_Pack of `incount` objects of `datatype` (typed -> packed),
+// us_out[1] an empty kernel launch + cudaStreamSynchronize on TEMPI's stream,
+// us_out[2] the empty launch alone, us_out[3] cudaStreamSynchronize of the
+// idle stream, us_out[4] cudaPointerGetAttributes of both buffers.  Each is
+// the median over 5 batches of `n` calls (after 200 untimed calls) of the
+// mean per call.
+int tempi_bench_call_overhead(int datatype, void *typed, void *packed,
+                              int incount, int capacity, int n,
+                              double *us_out) {
+  if (n < 1 || !us_out)
+    return 1;
+  cudaStream_t s = static_cast<cudaStream_t>(tempi_stream());
+  int err = 0;
+  auto per_call = [&](auto f) {
+    for (int i = 0; i < 200; ++i)
+      f();
+    double v[5];
+    for (double &x : v) {
+      const auto t0 = std::chrono::steady_clock::now();
+      for (int i = 0; i < n; ++i)
+        f();
+      x = std::chrono::duration<double, std::micro>(
+              std::chrono::steady_clock::now() - t0)
+              .count() /
+          n;
+    }
+    std::sort(v, v + 5);
+    return v[2];
+  };
+  us_out[0] = per_call([&] {
+    int pos = 0;
+    if (MPI_Pack(typed, incount, datatype, packed, capacity, &pos,
+                 MPI_COMM_WORLD) != MPI_SUCCESS)
+      err = 2;
+  });
+  us_out[1] = per_call([&] {
+    k_bench_empty<<<1, 32, 0, s>>>();
+    if (cudaStreamSynchronize(s) != cudaSuccess)
+      err = 2;
+  });
+  us_out[2] = per_call([&] { k_bench_empty<<<1, 32, 0, s>>>(); });
+  if (cudaStreamSynchronize(s) != cudaSuccess)
+    err = 2;
+  us_out[3] = per_call([&] { cudaStreamSynchronize(s); });
+  us_out[4] = per_call([&] {
+    cudaPointerAttributes a, b;
+    cudaPointerGetAttributes(&a, typed);
+    cudaPointerGetAttributes(&b, packed);
+  });
+  return err ? err : (cudaGetLastError() == cudaSuccess ? 0 : 2);
 }
 
 int tempi_bench_flush(void *buf, size_t bytes, void *stream) {

@@ -258,3 +258,101 @@ def test_reference_kernels_on_the_sweep(cuda, mpi_init, ref):
     if out and os.path.isdir(out):
         with open(os.path.join(out, "ref_kernels_sweep.json"), "w") as f:
             json.dump(rows, f, indent=1)
+
+
+def test_reference_kernels_on_the_halo(cuda, mpi_init, ref):
+    """The 256^3 grid of doubles at radius 2: its 26 send regions packed by
+    the reference's packer (one pack_3d launch per region, as the reference's
+    MPI_Pack runs them, without the synchronisation after each), by this
+    library's plain kernels (one launch per region, the learned picks) and by
+    one batched launch, on the same buffers; and the oracle's C walker on one
+    host core over the same regions (the CPU baseline).  All write the same
+    bytes.  Each GPU sequence is timed with CUDA events around its launches,
+    the L2 flushed before each, median of 5.  Results go to
+    $TEMPI_RESULTS_DIR/halo_ref_kernels.json when set."""
+    import statistics
+    import sys
+    import time
+
+    import torch
+
+    from oracle import walker as W
+    from tempi_b200 import halo
+
+    sys.path.insert(0, ROOT)
+    from bench import learned_configs
+
+    lib = _lib.tempi()
+    g = halo.Grid((256, 256, 256), 2)
+    gen = torch.Generator(device="cuda").manual_seed(33)
+    data = torch.randint(0, 256, (g.nbytes,), dtype=torch.uint8, device="cuda", generator=gen)
+    packs = {k: torch.zeros(g.packed_bytes, dtype=torch.uint8, device="cuda")
+             for k in ("reference", "plain", "batched")}
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    offs = g.offsets()
+    sizes = [g.alloc[2], g.alloc[1], g.alloc[0]]
+    plan = []
+    for d in halo.directions():
+        subs, starts = g.region_shape[(d, False)]
+        o = T.subarray(sizes, subs, starts, T.ORDER_C, T.named(8))
+        sb = R.canonicalize(o)
+        assert sb.ndims == 3  # no region spans a full row of the grid
+        # the reference's word size (from block and start) divides every
+        # stride and packed offset here, so its kernel is correct
+        assert sb.strides[1] % 8 == 0 and sb.strides[2] % 8 == 0 and offs[d] % 8 == 0
+        err, desc = mpi.describe(g.send[d])
+        assert err == 0
+        cp, _ = learned_configs(lib, desc, 1)
+        plan.append((d, o, sb, desc, cp))
+    batch = halo.HaloBatch([g], [data.data_ptr()], [packs["batched"].data_ptr()])
+
+    def run(who):
+        p = packs[who]
+        if who == "batched":
+            batch.launch()
+            return
+        for d, _, sb, desc, cp in plan:
+            dst = p.data_ptr() + offs[d]
+            if who == "reference":
+                assert ref_launch(ref, sb, 0, data.data_ptr(), dst, 1) == 0
+            else:
+                _lib.check(lib.tempi_pack(ctypes.byref(desc), data.data_ptr(), 1, dst,
+                                          ctypes.byref(cp) if cp else None, None))
+
+    times = {}
+    for who in ("reference", "plain", "batched"):
+        run(who)
+        ts = []
+        for _ in range(5):
+            flush.fill_(1)
+            flush.view(torch.int64).sum()
+            e0, e1 = _events()
+            e0.record()
+            run(who)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) * 1e3)
+        times[who] = statistics.median(ts)
+    torch.cuda.synchronize()
+    assert torch.equal(packs["reference"], packs["plain"])
+    assert torch.equal(packs["batched"], packs["plain"])
+    batch.close()
+
+    host = data.cpu().numpy()
+    walkers = [(d, W.Walker(o)) for d, o, _, _, _ in plan]
+    cpu = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        out = np.concatenate([w.pack(host, 1, nthreads=1) for _, w in walkers])
+        cpu.append((time.perf_counter() - t0) * 1e6)
+    assert np.array_equal(out, packs["plain"].cpu().numpy())
+    row = {"grid": "256^3 doubles, radius 2, 26 regions", "packed_bytes": g.packed_bytes,
+           "reference_26_launches_us": round(times["reference"], 1),
+           "tempi_26_launches_us": round(times["plain"], 1),
+           "tempi_batched_us": round(times["batched"], 1),
+           "oracle_c_walker_1_core_us": round(statistics.median(cpu), 1)}
+    print(json.dumps(row))
+    res = os.environ.get("TEMPI_RESULTS_DIR", "")
+    if res and os.path.isdir(res):
+        with open(os.path.join(res, "halo_ref_kernels.json"), "w") as f:
+            json.dump(row, f, indent=1)
