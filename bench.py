@@ -1044,7 +1044,9 @@ def dispatch_sample(torch, n=200, seed=777):
     timed again (the noise ceiling of the within-5 % figure), and the learned
     pick is also scored on the mean of the two measurements (the
     `_two_measurements` figures), which halves the variance of each
-    candidate's time."""
+    candidate's time.  The `deployed_` figures score what MPI_Type_commit
+    actually runs: the model's pick where the ensemble's spread is within
+    TEMPI_DISPATCH_SPREAD, else a measurement's fastest candidate."""
     from tempi_b200 import _lib
     from tempi_b200 import dispatch_train as DT
 
@@ -1053,7 +1055,11 @@ def dispatch_sample(torch, n=200, seed=777):
     times = (ctypes.c_float * DT.N_MEAS)()
     times2 = (ctypes.c_float * DT.N_MEAS)()
     learned, fixed, best, where, rep_best, rep_self = [], [], [], [], [], []
-    learned_m, best_m = [], []
+    learned_m, best_m, deployed, untrusted, sweep_lim = [], [], [], [], []
+    spr = (ctypes.c_float * DT.N_OUT)()
+    # the library's TEMPI_DISPATCH_SPREAD (default 0.5 in log2): above it,
+    # MPI_Type_commit measures the candidates instead of trusting the model
+    limit = float(os.environ.get("TEMPI_DISPATCH_SPREAD", "0.5"))
     t0 = time.time()
     while len(best) < n and time.time() - t0 < 90:
         d, incount, th, ph = DT.random_layout(rng)
@@ -1066,7 +1072,7 @@ def dispatch_sample(torch, n=200, seed=777):
         pc, uc, mi = ctypes.c_int(-1), ctypes.c_int(-1), ctypes.c_int(0)
         if lib.tempi_dispatch_choose(ctypes.byref(d), incount, int(th), int(ph), 0,
                                      ctypes.byref(pc), ctypes.byref(uc), ctypes.byref(mi),
-                                     None, None):
+                                     None, spr):
             return {"error": _lib.last_error()}
         t = np.frombuffer(times, np.float32)
         t2 = np.frombuffer(times2, np.float32)
@@ -1083,10 +1089,33 @@ def dispatch_sample(torch, n=200, seed=777):
         mp, mu = (tp + tp2) / 2, (tu + tu2) / 2
         best_m.append(float(np.nanmin(mp) + np.nanmin(mu)))
         learned_m.append(float(mp[pc.value] + mu[uc.value]))
+        # the deployed policy: the model's pick where the ensemble agrees,
+        # else a measurement's fastest (the first one here), scored on the
+        # second measurement against its own fastest
+        tr_p = spr[DT.PACK + pc.value] <= limit
+        tr_u = spr[DT.UNPACK + uc.value] <= limit
+        dp = pc.value if tr_p else int(np.nanargmin(tp))
+        du = uc.value if tr_u else int(np.nanargmin(tu))
+        deployed.append(float(tp2[dp] + tu2[du]))
+        untrusted.append(not (tr_p and tr_u))
+        # for other spread limits: the spreads of both picks and the
+        # second measurement's times of the model's and the measured picks
+        sweep_lim.append((spr[DT.PACK + pc.value], spr[DT.UNPACK + uc.value],
+                          float(tp2[pc.value]), float(tp2[int(np.nanargmin(tp))]),
+                          float(tu2[uc.value]), float(tu2[int(np.nanargmin(tu))])))
         where.append((d.as_dict(), incount, bool(th), bool(ph), pc.value, uc.value))
     L, F, B = map(np.array, (learned, fixed, best))
     RS, RB = np.array(rep_self), np.array(rep_best)
     LM, BM = np.array(learned_m), np.array(best_m)
+    DP = np.array(deployed)
+    by_limit = {}
+    for lim in (0.1, 0.2, 0.3, 0.5, 1.0):
+        d = np.array([(a if sa <= lim else b) + (c if su <= lim else e)
+                      for sa, su, a, b, c, e in sweep_lim])
+        meas = np.mean([not (sa <= lim and su <= lim) for sa, su, *_ in sweep_lim])
+        by_limit[str(lim)] = {"within_5pct": round(float(np.mean(d <= 1.05 * RB)), 3),
+                              "total_regret": round(float(d.sum() / RB.sum() - 1), 4),
+                              "measured_fraction": round(float(meas), 3)}
     worst = [{"us_learned": round(float(L[i]), 1), "us_best": round(float(B[i]), 1),
               "layout": where[i][0], "incount": where[i][1], "typed_host": where[i][2],
               "packed_host": where[i][3], "picks": where[i][4:]}
@@ -1098,6 +1127,10 @@ def dispatch_sample(torch, n=200, seed=777):
             "learned_mean_regret": round(float(np.mean(L / B - 1)), 4),
             "learned_within_5pct_two_measurements": round(float(np.mean(LM <= 1.05 * BM)), 3),
             "learned_total_regret_two_measurements": round(float(LM.sum() / BM.sum() - 1), 4),
+            "deployed_within_5pct": round(float(np.mean(DP <= 1.05 * RB)), 3),
+            "deployed_total_regret": round(float(DP.sum() / RB.sum() - 1), 4),
+            "deployed_measured_fraction": round(float(np.mean(untrusted)), 3),
+            "deployed_by_spread_limit": by_limit,
             "exhaustive_repeat_within_5pct": round(float(np.mean(RS <= 1.05 * RB)), 3),
             "exhaustive_repeat_total_regret": round(float(RS.sum() / RB.sum() - 1), 4),
             "exhaustive_total_us": round(float(B.sum()), 1),
