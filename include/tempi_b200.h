@@ -78,17 +78,22 @@ typedef struct tempi_desc {
 /* Kernel choice for one launch.  Zero fields mean "let the library pick".
    kernel: 0 auto, 1 word kernel (a thread per vector word), 2 row kernel (a
    warp per row), 3 shift kernel (a group of `unroll` = 4/8/16/32 lanes per
-   row, 16-B accesses at any alignment), 4 staged kernels (8 KB chunks of the
-   packed stream move through shared memory by bulk asynchronous copies, 3 in
-   flight per block: an unpack pulls packed chunks in and scatters them by
-   vector words, and needs a 16-B aligned packed base and a packed size that
-   is a multiple of 16; a pack gathers row pieces in and writes them out in
-   16-B words, and needs width 16 throughout.  Both need device memory on
-   both sides; calls that do not qualify take the automatic rules).  width:
-   vector bytes for kernels 1, 2 and 4 (1,2,4,8,16; never above what the
-   alignment proof allows).  blocks_per_sm: resident blocks per SM the grid
-   is sized for (kernel 4: 1..8, default 3 for aligned copies of 32 MiB or
-   more, else 8). */
+   row, 16-B accesses at any alignment), 4 staged kernels (chunks of the packed
+   stream move through shared memory by bulk asynchronous copies: a pack
+   gathers 16 KB chunks' row pieces in and writes each chunk out with one
+   bulk store, and needs width 16 throughout; an unpack needs a 16-B aligned
+   packed base, and for 16-B aligned rows of 512 B or more (or one
+   contiguous run) pulls 16 KB chunks in and writes their row pieces out
+   with bulk stores, else pulls 8 KB chunks in and scatters them by vector
+   words.  Every staged launch needs a packed size that is a multiple
+   of 16 and device memory on both sides; calls that do not qualify take the
+   automatic rules).  width: vector bytes for kernels 1, 2 and 4
+   (1,2,4,8,16; never above what the alignment proof allows).
+   blocks_per_sm: resident blocks per SM the grid is sized for (kernel 4:
+   1..8; the 16 KB-chunk kernels run one warp per block, one block per SM
+   for 96 MiB or more and 3 below, and blocks_per_sm only lowers that; the
+   scattering unpack defaults to 3 for aligned copies of 32 MiB or more,
+   else 8). */
 typedef struct tempi_config {
   int32_t kernel;
   int32_t width;

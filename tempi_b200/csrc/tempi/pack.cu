@@ -24,9 +24,13 @@
 //    wide rows.
 //  * k_rows_shift: a group of lanes per row, 16-B words realigned by funnel
 //    shifts, for rows whose two sides disagree modulo 16.
-//  * k_pack_staged / k_unpack_staged: 8 KB chunks of the packed stream move
-//    between global and shared memory by bulk asynchronous copies counted on
-//    mbarriers (bounded waits), the other side by coalesced plain accesses.
+//  * k_unpack_staged: 8 KB chunks of the packed stream move into shared
+//    memory by bulk asynchronous copies counted on mbarriers (bounded
+//    waits), and are scattered to the rows by plain vector stores.
+//  * k_staged_bulk: the staged pack, and the staged unpack of wide 16-B
+//    aligned rows: one warp per CTA moves 16 KB chunks through shared memory
+//    with bulk copies in both directions (row pieces on the strided side,
+//    one copy on the packed side).
 //  * grids are a multiple of the SM count and grid-stride over the work.
 
 #include "internal.hpp"
@@ -36,6 +40,8 @@
 #include <atomic>
 #include <cstring>
 #include <mutex>
+#include <set>
+#include <utility>
 
 namespace tempi {
 
@@ -348,6 +354,27 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar,
   return true;
 }
 
+// mbarrier.try_wait suspends the thread until the phase completes or a
+// hardware time limit passes, so a waiting warp neither spins nor sleeps
+// past the completion; false after about 2^31 SM cycles (about a second)
+__device__ __forceinline__ bool mbar_try_wait_bounded(uint64_t *bar,
+                                                      uint32_t parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    if (ok)
+      return true;
+    if (clock64() - t0 > (1ll << 31))
+      return false;
+  }
+}
+
 // The give-up path of a staged CTA, run by one thread: report the failure,
 // then wait once more (bounded again) on every stage that still has copies
 // counted -- the stage whose wait ran out included -- so that a copy that
@@ -428,108 +455,201 @@ __global__ void __launch_bounds__(kStagedThreads)
   }
 }
 
-// The staged pack: the mirror of k_unpack_staged for geometries whose every
-// row, stride and base is 16-B aligned (width 16).  Chunk c of the packed
-// stream is gathered into shared memory by one bulk copy per row piece it
-// covers -- the lanes of warp 0 issue the pieces in parallel, all counted on
-// the chunk's mbarrier -- and the threads then write the chunk to the packed
-// buffer with coalesced 16-B stores.  Same bounded waits and give-up path as
-// the staged unpack.
-template <int ND>
-__global__ void __launch_bounds__(kStagedThreads)
-    k_pack_staged(const char *__restrict__ strided, char *__restrict__ packed,
+// The bulk kernels: the staged pack, and the staged unpack of 16-B aligned
+// rows of at least kBulkMinRow bytes (or of a contiguous run).  One warp per
+// CTA moves kBulkChunk-byte chunks of the packed stream through kBulkStages
+// shared-memory stages with bulk asynchronous copies in both directions, and
+// no thread touches the data:
+//   pack    the row pieces of chunk c are gathered into a stage (one bulk
+//           copy per piece, the lanes issuing pieces in parallel, all
+//           counted on the stage's mbarrier); lane 0 writes the stage to
+//           the packed buffer with one bulk store;
+//   unpack  lane 0 pulls chunk c into a stage with one bulk copy; the lanes
+//           write its row pieces out with one bulk store each.
+// A stage is refilled once the bulk stores that read it have finished
+// reading (cp.async.bulk.wait_group.read), one iteration behind, so
+// kBulkStages - 1 chunks are on their way in while one goes out.  Every
+// piece is 16-B aligned with a multiple of 16 bytes (width 16: block,
+// strides and both bases), as bulk copies require.  Each wait on an
+// mbarrier is bounded as in k_unpack_staged; a CTA that gives up sets the
+// failure word, waits (bounded) on every chunk it has requested, waits for
+// its stores and returns.
+constexpr uint32_t kBulkChunk = 16384;
+constexpr int kBulkStages = 4;
+constexpr int kBulkSmem = int(kBulkChunk) * kBulkStages;
+constexpr int kBulkMaxPerSm = 3;       // 3 x 64 KB of shared memory per SM
+constexpr uint64_t kBulkMinRow = 512;  // narrower unpacks scatter by words
+// Measured on B200, contiguous copies back to back: one CTA per SM moves 128
+// MiB and more 3-4 % faster than two or three (fewer interleaved streams),
+// while below that the extra CTAs win (64 MiB: 21.0 us at 2-3 per SM
+// against 25.0 at one)
+constexpr uint64_t kBulkOnePerSm = uint64_t(96) << 20;
+
+__device__ __forceinline__ void bulk_expect(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                   smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// global -> shared, completion counted on `bar`
+__device__ __forceinline__ void bulk_in(void *dst, const void *src,
+                                        uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::"
+               "bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// shared -> global, in this thread's current bulk group
+__device__ __forceinline__ void bulk_out(void *dst, const void *src,
+                                         uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::
+                   "l"(dst),
+               "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+}
+
+template <int ND, bool UNPACK>
+__global__ void __launch_bounds__(32)
+    k_staged_bulk(char *__restrict__ strided, char *__restrict__ packed,
                   const __grid_constant__ Geometry g, uint32_t nchunks,
                   uint64_t total_bytes, StagedCtl ctl) {
-  __shared__ __align__(128) char stage[kStagedStages][kStagedBytes];
-  __shared__ __align__(8) uint64_t bar[kStagedStages];
-  __shared__ int gave_up;
+  extern __shared__ __align__(128) char stage[]; // kBulkStages x kBulkChunk
+  __shared__ __align__(8) uint64_t bar[kBulkStages];
+  const uint32_t lane = threadIdx.x;
   const uint64_t block = uint64_t(g.block);
   auto chunk_bytes = [&](uint32_t c) {
-    const uint64_t left = total_bytes - uint64_t(c) * kStagedBytes;
-    return uint32_t(left < uint64_t(kStagedBytes) ? left : kStagedBytes);
+    const uint64_t left = total_bytes - uint64_t(c) * kBulkChunk;
+    return uint32_t(left < uint64_t(kBulkChunk) ? left : kBulkChunk);
   };
-  // warp 0 only: the row pieces of chunk c into stage s
-  auto gather = [&](uint32_t c, int s) {
-    const uint32_t lane = threadIdx.x;
-    const uint64_t p0 = uint64_t(c) * kStagedBytes;
+  // piece k of chunk c (lane l takes k = l, l + 32, ...): stage bytes
+  // [d, d + len) and the strided bytes of row row0 + k from offset o
+  auto pieces = [&](uint32_t c, auto &&f) {
+    const uint64_t p0 = uint64_t(c) * kBulkChunk;
     const uint32_t n = chunk_bytes(c);
-    if (lane == 0)
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::
-                       "r"(smem_u32(&bar[s])),
-                   "r"(n + ctl.shortfall)
-                   : "memory");
-    __syncwarp();
     const uint32_t row0 = uint32_t(p0 / block);
     const uint64_t off0 = p0 - uint64_t(row0) * block;
     const uint64_t first = block - off0; // bytes of the first row's piece
     for (uint32_t k = lane;; k += 32) {
-      // piece k: row row0 + k, at chunk offset d, in-row offset o
       const uint64_t d = k == 0 ? 0 : first + uint64_t(k - 1) * block;
       if (d >= n)
         break;
       const uint64_t o = k == 0 ? off0 : 0;
       const uint64_t len = block - o < n - d ? block - o : n - d;
-      asm volatile(
-          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
-          " [%0], [%1], %2, [%3];" ::"r"(smem_u32(stage[s] + d)),
-          "l"(strided + row_offset<ND>(row0 + k, g) + o), "r"(uint32_t(len)),
-          "r"(smem_u32(&bar[s]))
-          : "memory");
+      f(uint32_t(d), strided + row_offset<ND>(row0 + k, g) + o, uint32_t(len));
     }
   };
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kStagedStages; ++s)
+  // warp-wide: chunk c into stage s
+  auto fill = [&](uint32_t c, int s) {
+    char *st = stage + size_t(s) * kBulkChunk;
+    if (lane == 0)
+      bulk_expect(&bar[s], chunk_bytes(c) + ctl.shortfall);
+    __syncwarp();
+    if (UNPACK) {
+      if (lane == 0)
+        bulk_in(st, packed + uint64_t(c) * kBulkChunk, chunk_bytes(c), &bar[s]);
+    } else {
+      pieces(c, [&](uint32_t d, const char *src, uint32_t len) {
+        bulk_in(st + d, src, len, &bar[s]);
+      });
+    }
+  };
+  // warp-wide: stage s out to where chunk c belongs, one bulk group per lane
+  auto empty = [&](uint32_t c, int s) {
+    const char *st = stage + size_t(s) * kBulkChunk;
+    if (UNPACK) {
+      pieces(c, [&](uint32_t d, char *dst, uint32_t len) {
+        bulk_out(dst, st + d, len);
+      });
+    } else if (lane == 0) {
+      bulk_out(packed + uint64_t(c) * kBulkChunk, st, chunk_bytes(c));
+    }
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  };
+  if (lane == 0) {
+    for (int s = 0; s < kBulkStages; ++s)
       mbar_init(&bar[s]);
-    gave_up = 0;
+    // the initialised barriers are visible to the copy engine's proxy
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __syncthreads();
-  if (threadIdx.x < 32)
-    for (int s = 0; s < kStagedStages; ++s) {
-      const uint32_t c = blockIdx.x + uint32_t(s) * gridDim.x;
-      if (c < nchunks)
-        gather(c, s);
-    }
+  __syncwarp();
+  uint32_t issued = 0; // iterations whose chunk has been requested
+  for (int s = 0; s < kBulkStages; ++s) {
+    const uint32_t c = blockIdx.x + uint32_t(s) * gridDim.x;
+    if (c >= nchunks)
+      break;
+    fill(c, s);
+    ++issued;
+  }
   uint32_t it = 0;
   for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x, ++it) {
-    const int s = int(it % kStagedStages);
-    const uint32_t parity = (it / kStagedStages) & 1;
-    if (!mbar_wait_bounded(&bar[s], parity))
-      gave_up = 1;
-    __syncthreads();
-    if (gave_up) {
-      if (threadIdx.x == 0)
-        staged_drain(ctl, bar, c, it, nchunks);
-      return;
+    const int s = int(it % kBulkStages);
+    const bool ok = mbar_try_wait_bounded(&bar[s], (it / kBulkStages) & 1);
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) {
+        staged_give_up(ctl);
+        for (uint32_t j = it; j < issued; ++j)
+          mbar_try_wait_bounded(&bar[j % kBulkStages], (j / kBulkStages) & 1);
+      }
+      __syncwarp();
+      break;
     }
-    const uint32_t words = chunk_bytes(c) / 16;
-    const uint4 *src = reinterpret_cast<const uint4 *>(stage[s]);
-    uint4 *dst = reinterpret_cast<uint4 *>(packed + uint64_t(c) * kStagedBytes);
-    for (uint32_t j = threadIdx.x; j < words; j += blockDim.x)
-      dst[j] = src[j];
-    __syncthreads(); // every thread is done with stage s
-    if (threadIdx.x < 32) {
-      const uint32_t cn = c + uint32_t(kStagedStages) * gridDim.x;
-      if (cn < nchunks)
-        gather(cn, s);
+    empty(c, s);
+    // the stage emptied one iteration ago is free once its stores have read
+    // it: refill it with the chunk kBulkStages - 1 iterations ahead
+    asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+    __syncwarp();
+    if (it >= 1) {
+      const uint32_t cn = c + uint32_t(kBulkStages - 1) * gridDim.x;
+      if (cn < nchunks) {
+        fill(cn, int((it - 1) % kBulkStages));
+        ++issued;
+      }
     }
   }
+  // every store complete before the CTA (and its shared memory) goes
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 using StagedFn = void (*)(char *, const char *, Geometry, uint32_t, uint64_t,
                           StagedCtl);
-using StagedPackFn = void (*)(const char *, char *, Geometry, uint32_t,
-                              uint64_t, StagedCtl);
+using BulkFn = void (*)(char *, char *, Geometry, uint32_t, uint64_t,
+                        StagedCtl);
 
-StagedPackFn pick_staged_pack(uint32_t nd) {
+template <bool UNPACK> BulkFn pick_bulk(uint32_t nd) {
   switch (nd) {
-  case 0: return k_pack_staged<0>;
-  case 1: return k_pack_staged<1>;
-  case 2: return k_pack_staged<2>;
-  case 3: return k_pack_staged<3>;
-  case 4: return k_pack_staged<4>;
-  default: return k_pack_staged<5>;
+  case 0: return k_staged_bulk<0, UNPACK>;
+  case 1: return k_staged_bulk<1, UNPACK>;
+  case 2: return k_staged_bulk<2, UNPACK>;
+  case 3: return k_staged_bulk<3, UNPACK>;
+  case 4: return k_staged_bulk<4, UNPACK>;
+  default: return k_staged_bulk<5, UNPACK>;
   }
+}
+
+// The bulk kernels take more than the default 48 KB of dynamic shared
+// memory; the limit is raised once per kernel and device.
+bool bulk_smem_ready(BulkFn fn) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  static std::mutex mu;
+  static std::set<std::pair<int, const void *>> done;
+  const auto key = std::make_pair(dev, reinterpret_cast<const void *>(fn));
+  std::lock_guard<std::mutex> l(mu);
+  if (done.count(key))
+    return true;
+  if (cudaFuncSetAttribute(reinterpret_cast<const void *>(fn),
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           kBulkSmem) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  done.insert(key);
+  return true;
 }
 
 // The failure word of the staged kernels: one int of mapped pinned host
@@ -822,30 +942,52 @@ int launch_geometry(const Geometry &g, const char *strided, char *packed,
   const bool wide = g.width == 16 && bytes >= (uint64_t(32) << 20);
   const bool narrow_unpack =
       unpack && bytes >= (uint64_t(1) << 20) && g.block <= 512;
-  if ((kernel == 4 || ((kernel < 1 || kernel > 4) && (wide || narrow_unpack))) &&
+  bool staged =
+      (kernel == 4 || ((kernel < 1 || kernel > 4) && (wide || narrow_unpack))) &&
       bytes % 16 == 0 &&
       (unpack ? (reinterpret_cast<uintptr_t>(packed) & 15) == 0
               : g.width == 16) &&
       (both_device >= 0
            ? both_device == 1
            : classify(strided).is_device && classify(packed).is_device) &&
-      staged_channel(stream)) {
-    const uint32_t nchunks =
-        uint32_t((bytes + kStagedBytes - 1) / kStagedBytes);
-    // measured on the strided sweep: 3 CTAs per SM for long aligned
-    // streams, a full SM (8 CTAs of 256 threads) for narrow scatters
-    const int bps = (cfg && cfg->blocks_per_sm >= 1 && cfg->blocks_per_sm <= 8)
-                        ? cfg->blocks_per_sm
-                        : wide ? 3 : 8;
-    const uint32_t blocks = std::max<uint32_t>(
-        1, std::min<uint32_t>(nchunks, uint32_t(sms) * uint32_t(bps)));
+      staged_channel(stream);
+  // packs, and unpacks of wide aligned rows, run the bulk kernels
+  BulkFn bulk = nullptr;
+  if (staged &&
+      (!unpack || (g.width == 16 && (g.nd == 0 || g.block >= kBulkMinRow)))) {
+    bulk = unpack ? pick_bulk<true>(g.nd) : pick_bulk<false>(g.nd);
+    if (!bulk_smem_ready(bulk)) {
+      bulk = nullptr;
+      staged = unpack; // a pack then takes the plain kernels
+    }
+  }
+  if (staged) {
     const StagedCtl ctl{g_fail_dev, uint32_t(env().staged_shortfall)};
-    if (unpack)
+    const int req =
+        (cfg && cfg->blocks_per_sm >= 1 && cfg->blocks_per_sm <= 8)
+            ? cfg->blocks_per_sm
+            : 0;
+    if (bulk) {
+      // one warp per CTA: one CTA per SM for long streams, else as many as
+      // their shared memory allows; a requested count caps it
+      const uint32_t nchunks = uint32_t((bytes + kBulkChunk - 1) / kBulkChunk);
+      const int own = bytes >= kBulkOnePerSm ? 1 : kBulkMaxPerSm;
+      const int bps = req ? std::min(req, own) : own;
+      const uint32_t blocks = std::max<uint32_t>(
+          1, std::min<uint32_t>(nchunks, uint32_t(sms) * uint32_t(bps)));
+      bulk<<<blocks, 32, kBulkSmem, stream>>>(const_cast<char *>(strided),
+                                               packed, g, nchunks, bytes, ctl);
+    } else {
+      const uint32_t nchunks =
+          uint32_t((bytes + kStagedBytes - 1) / kStagedBytes);
+      // measured on the strided sweep: 3 CTAs per SM for long aligned
+      // streams, a full SM (8 CTAs of 256 threads) for narrow scatters
+      const int bps = req ? req : wide ? 3 : 8;
+      const uint32_t blocks = std::max<uint32_t>(
+          1, std::min<uint32_t>(nchunks, uint32_t(sms) * uint32_t(bps)));
       pick_staged(g.width, g.nd)<<<blocks, kStagedThreads, 0, stream>>>(
           const_cast<char *>(strided), packed, g, nchunks, bytes, ctl);
-    else
-      pick_staged_pack(g.nd)<<<blocks, kStagedThreads, 0, stream>>>(
-          strided, packed, g, nchunks, bytes, ctl);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
       return cuda_error(e, "staged kernel launch");

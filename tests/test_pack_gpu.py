@@ -584,7 +584,11 @@ def test_staged_unpack_matches_oracle(cuda, mpi_init):
         (_lib.Desc.make(120, 300 * 1024, 64, [17, 300], [1024, 17 * 1024]), 1),
         (_lib.Desc.make(3, 70000, 48, [1200], [57]), 1),
         (_lib.Desc.make(2, 14000, 32, [5, 7, 9], [34, 200, 1500]), 3),
+        # 16-B aligned rows of 512 B and more, and a contiguous run: the bulk
+        # kernel (bulk stores per row piece; partial last chunks)
         (_lib.Desc.make(0, 1 << 20, 4096, [60], [8192]), 2),
+        (_lib.Desc.make(16, 200 * 2080 + 64, 528, [13, 15], [1040, 13 * 1040 + 48]), 3),
+        (_lib.Desc.make(32, (3 << 20) + 1296, (3 << 20) + 1264, [], []), 2),
     ]
     before = _lib.counter("staged_timeouts")
     for d, incount in cases:
@@ -616,7 +620,7 @@ def test_staged_unpack_matches_oracle(cuda, mpi_init):
 
 def test_staged_pack_matches_oracle(cuda, mpi_init):
     """The staged pack (kernel 4 on the pack side: row pieces gathered into
-    shared memory by bulk copies, written out with coalesced stores) on
+    shared memory by bulk copies, written out by bulk stores) on
     16-B aligned geometries: rows of 16 B (hundreds of pieces per chunk),
     rows that chunks cut in the middle, a contiguous run with a partial last
     chunk, and enough chunks that each CTA cycles its stages several times
@@ -838,3 +842,59 @@ def test_staged_give_up_is_reported(cuda, mpi_init):
     assert err == 0 and host(dst).tobytes() == exp.tobytes()
     assert _lib.counter("staged_timeouts") == before + 2
     mpi.Type_free(t)
+
+
+@pytest.mark.parametrize("unpack", [0, 1])
+def test_bulk_give_up_is_reported(cuda, mpi_init, unpack):
+    """The bulk kernels (the staged pack, and the staged unpack of wide
+    aligned rows) under TEMPI_TEST_STAGED_SHORTFALL: every chunk's barrier
+    expects 16 bytes more than its copies bring, so each bounded wait gives
+    up; the launch reports TEMPI_ERR_TIMEOUT once, and the same call on the
+    same context is exact once the knob is cleared."""
+    import os
+
+    import torch
+
+    from tests.test_canon import desc_pack
+
+    lib = _lib.tempi()
+    # 1 MiB packed in rows of 1 KiB, 16-B aligned: 64 chunks of 16 KB, one
+    # per CTA, so each CTA waits once and drains one chunk
+    d = _lib.Desc.make(0, 1 << 21, 1024, [1024], [2048])
+    span = d.block + d.strides[0] * (d.counts[0] - 1)
+    src_np = H.splitmix_bytes(span, 91)
+    want = desc_pack(d, src_np, 1)
+    exp = np.full(span, 0xAA, np.uint8)
+    T.unpack(T.hvector(1024, 1024, 2048, T.BYTE), want, exp, 1)
+    cfg = _lib.Config(4, 0, 256, 0, 3, 0)
+    src = torch.from_numpy(src_np).cuda()
+    packed = torch.from_numpy(want).cuda()
+
+    def run():
+        if unpack:
+            out = torch.full((span,), 0xAA, dtype=torch.uint8, device="cuda")
+            _lib.check(lib.tempi_unpack(ctypes.byref(d), packed.data_ptr(), 1, out.data_ptr(),
+                                        ctypes.byref(cfg), None))
+        else:
+            out = torch.zeros(want.size, dtype=torch.uint8, device="cuda")
+            _lib.check(lib.tempi_pack(ctypes.byref(d), src.data_ptr(), 1, out.data_ptr(),
+                                      ctypes.byref(cfg), None))
+        sync()
+        assert lib.tempi_last_kernel().decode().startswith("staged")
+        return host(out)
+
+    before = _lib.counter("staged_timeouts")
+    assert lib.tempi_staged_check() == 0
+    os.environ["TEMPI_TEST_STAGED_SHORTFALL"] = "16"
+    try:
+        lib.tempi_reload_env()
+        run()
+        assert lib.tempi_staged_check() == 4  # TEMPI_ERR_TIMEOUT
+        assert lib.tempi_staged_check() == 0  # reported once
+        assert _lib.counter("staged_timeouts") == before + 1
+    finally:
+        del os.environ["TEMPI_TEST_STAGED_SHORTFALL"]
+        lib.tempi_reload_env()
+    got = run()
+    assert lib.tempi_staged_check() == 0
+    assert got.tobytes() == (exp if unpack else want).tobytes()
