@@ -404,17 +404,20 @@ tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
     return tempi_config{};
   const uint64_t key = config_key(incount, src_host, dst_host, unpack);
   const int lo = unpack ? kUnpackOut : kPackOut;
+  {
+    std::lock_guard<std::mutex> l(g_mu);
+    auto it = r.configs.find(key); // every call after the first: no strings
+    if (it != r.configs.end()) {
+      counters().dispatch_hit++;
+      return it->second < 0 ? tempi_config{} : kCandidates[it->second];
+    }
+  }
   const std::string lkey =
       layout_key(r.desc, incount, src_host, dst_host, unpack ? 'u' : 'p');
   const std::string lkey2 =
       layout_key(r.desc, incount, src_host, dst_host, unpack ? 'p' : 'u');
   {
     std::lock_guard<std::mutex> l(g_mu);
-    auto it = r.configs.find(key);
-    if (it != r.configs.end()) {
-      counters().dispatch_hit++;
-      return it->second < 0 ? tempi_config{} : kCandidates[it->second];
-    }
     auto lt = g_layouts.find(lkey); // another handle of the same layout
     if (lt != g_layouts.end()) {
       counters().dispatch_hit++;
