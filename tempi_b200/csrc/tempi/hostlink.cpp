@@ -113,7 +113,9 @@ int host_link_copy(void *dst, const void *src, size_t n, cudaStream_t s) {
   // at least 2 * kStages chunks so both directions overlap for most of it;
   // whole MiB, so every staging slot and chunk offset stays aligned
   const size_t want = (n / (2 * kStages) + kMinChunk - 1) / kMinChunk * kMinChunk;
-  const size_t chunk = std::min(kMaxChunk, std::max(kMinChunk, want));
+  const size_t chunk = env().host_link_chunk_kb > 0
+                           ? size_t(env().host_link_chunk_kb) << 10
+                           : std::min(kMaxChunk, std::max(kMinChunk, want));
   const char *sp = static_cast<const char *>(src);
   char *dp = static_cast<char *>(dst);
   return pipeline(

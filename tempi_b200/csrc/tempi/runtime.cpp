@@ -52,6 +52,9 @@ void read_env() {
     e.wait_timeout_s = std::atof(s);
   if (const char *s = std::getenv("TEMPI_HOST_LINK"))
     e.host_link_dma = std::string(s) != "kernel";
+  if (const char *s = std::getenv("TEMPI_HOST_LINK_CHUNK_KB"))
+    e.host_link_chunk_kb =
+        std::max(0L, std::min(65536L, std::atol(s))) / 256 * 256;
   if (const char *s = std::getenv("TEMPI_TEST_STAGED_SHORTFALL"))
     e.staged_shortfall = std::max(0, std::min(4096, std::atoi(s))) & ~15;
   if (has("TEMPI_ALLTOALLV_REMOTE_FIRST"))

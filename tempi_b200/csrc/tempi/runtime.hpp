@@ -31,6 +31,9 @@ struct Env {
   // TEMPI_HOST_LINK=kernel: contiguous runs between pinned host buffers go
   // through the kernels too, instead of the copy-engine pipeline
   bool host_link_dma = true;
+  // TEMPI_HOST_LINK_CHUNK_KB: chunk size of the copy-engine pipeline for
+  // contiguous runs, a multiple of 256 KiB (0: the built-in rule)
+  long host_link_chunk_kb = 0;
   // TEMPI_TEST_STAGED_SHORTFALL=<bytes>: the staged kernels' barriers expect
   // that many bytes per chunk beyond what their copies deliver, so every
   // bounded wait runs out (about a second) and the give-up path reports a
