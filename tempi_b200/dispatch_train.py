@@ -97,6 +97,11 @@ def span_of(desc, incount):
     return hi
 
 
+# back-to-back launches per candidate for objects under 1 MiB, under 64 MiB,
+# and larger (their mean is the label)
+REPS = (12, 6, 2)
+
+
 def measure_dataset(n, budget_s, seed, method_every=8, log=print):
     lib = _lib.tempi()
     rng = np.random.default_rng(seed)
@@ -117,7 +122,7 @@ def measure_dataset(n, budget_s, seed, method_every=8, log=print):
         # 64 MiB (host-staged transfers of larger objects take too long)
         methods = done % method_every == 0 and not th and not ph and size <= (64 << 20)
         what = 1 | (2 if methods else 0)
-        reps = 3 if size < (1 << 20) else 2 if size < (64 << 20) else 1
+        reps = REPS[0] if size < (1 << 20) else REPS[1] if size < (64 << 20) else REPS[2]
         err = lib.tempi_measure(ctypes.byref(d), incount, int(th), int(ph), what, reps, times)
         if err:
             raise RuntimeError(f"tempi_measure failed: {_lib.last_error()}")
@@ -349,9 +354,15 @@ def main(argv=None):
     ap.add_argument("--members", type=int, default=5)
     ap.add_argument("--epochs", type=int, default=None)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--reps", default=None,
+                    help="launches per candidate under 1 MiB,64 MiB,above (default 12,6,2)")
     ap.add_argument("--no-install", action="store_true",
                     help="do not write tempi_b200/models/")
     args = ap.parse_args(argv)
+    global REPS
+    if args.reps:
+        REPS = tuple(int(x) for x in args.reps.split(","))
+        assert len(REPS) == 3 and min(REPS) >= 1
     out = args.out or os.path.join(os.environ.get("TEMPI_CACHE_DIR", "."), "dispatch")
     os.makedirs(out, exist_ok=True)
     assert mpi.Init() == 0
@@ -400,7 +411,7 @@ def main(argv=None):
         "measure_s": round(t_meas, 1), "train_s": round(t_train, 2), "epochs": epochs,
         "members": args.members, "loss_first_epoch": float(losses[:, 0].mean()),
         "loss_last_epoch": float(losses[:, -1].mean()),
-        "seed": args.seed,
+        "seed": args.seed, "reps": list(REPS),
     })
     with open(os.path.join(out, "dispatch_report.json"), "w") as fh:
         json.dump(report, fh, indent=1)
