@@ -225,6 +225,37 @@ def test_host_to_host_contiguous_run(cuda, mpi_init, path, shape):
         _lib.tempi().tempi_reload_env()
 
 
+def test_host_link_small_chunks(cuda, mpi_init):
+    """The copy-engine pipeline with TEMPI_HOST_LINK_CHUNK_KB=256: a contiguous
+    run of 9 MiB + 12 B between pinned host buffers goes through 37 chunks,
+    each of the 4 staging slots reused 9 times, with a short last chunk; the
+    pack and the unpack write the oracle's bytes and nothing else."""
+    import os
+
+    import torch
+
+    ty = H.contiguous((9 << 20) // 4 + 3, H.named("FLOAT")).commit()
+    os.environ["TEMPI_HOST_LINK_CHUNK_KB"] = "256"
+    _lib.tempi().tempi_reload_env()
+    try:
+        src_np = H.splitmix_bytes(ty.o.extent, 41)
+        src = torch.from_numpy(src_np).pin_memory()
+        packed = torch.zeros(ty.o.size + 16, dtype=torch.uint8).pin_memory()
+        n0 = _lib.counter("host_link_copies")
+        err, pos = mpi.Pack(src.data_ptr(), 1, ty.h, packed.data_ptr(), packed.numel(), 16)
+        assert err == 0 and pos == 16 + ty.o.size
+        assert packed.numpy()[16:].tobytes() == src_np.tobytes()
+        assert not packed.numpy()[:16].any()
+        back = torch.full_like(src, 0xAA).pin_memory()
+        err, upos = mpi.Unpack(packed.data_ptr(), packed.numel(), back.data_ptr(), 1, ty.h, 16)
+        assert err == 0 and upos == pos
+        assert back.numpy().tobytes() == src_np.tobytes()
+        assert _lib.counter("host_link_copies") - n0 == 2
+    finally:
+        del os.environ["TEMPI_HOST_LINK_CHUNK_KB"]
+        _lib.tempi().tempi_reload_env()
+
+
 @pytest.mark.parametrize("path", ["dma", "kernel"])
 @pytest.mark.parametrize("shape", ["rows256_odd", "rows1000", "rows64_odd", "two_dims"])
 def test_host_to_host_strided_rows(cuda, mpi_init, path, shape):
