@@ -307,7 +307,8 @@ const char *tempi_last_kernel(void);
    "lib_pack", "lib_unpack", "cached_types", "send_device", "send_oneshot",
    "send_staged", "send_lib", "recv_device", "recv_oneshot", "recv_staged",
    "recv_lib", "isend_managed", "irecv_managed", "dispatch_hit",
-   "dispatch_miss", "slab_hits", "slab_misses", "slab_bytes" (bytes of
+   "dispatch_miss", "dispatch_measured" (kernel choices made by timing the
+   candidates: the exhaustive fallback), "slab_hits", "slab_misses", "slab_bytes" (bytes of
    slabs held from CUDA), "slab_live_bytes" (handed out), "slab_cached_bytes"
    (kept for reuse, at most TEMPI_SLAB_CACHE_MB per memory space),
    "host_link_copies", "send_contig_staged", "recv_contig_staged",

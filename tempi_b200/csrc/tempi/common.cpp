@@ -82,7 +82,7 @@ extern "C" int64_t tempi_counter(const char *name) {
   C(lib_pack) C(lib_unpack) C(cached_types) C(send_device) C(send_oneshot)
   C(send_staged) C(send_lib) C(recv_device) C(recv_oneshot) C(recv_staged)
   C(recv_lib) C(isend_managed) C(irecv_managed) C(dispatch_hit)
-  C(dispatch_miss) C(slab_hits) C(slab_misses) C(slab_bytes) C(slab_live_bytes) C(slab_cached_bytes) C(host_link_copies)
+  C(dispatch_miss) C(dispatch_measured) C(slab_hits) C(slab_misses) C(slab_bytes) C(slab_live_bytes) C(slab_cached_bytes) C(host_link_copies)
   C(send_contig_staged) C(recv_contig_staged) C(neighbor_fused)
   C(neighbor_isir) C(neighbor_lib) C(alltoallv_staged) C(alltoallv_remote_first)
   C(alltoallv_isir_staged) C(alltoallv_isir_remote_staged) C(alltoallv_lib)

@@ -284,6 +284,41 @@ int pick(const float *mean, const float *spread, int lo, int hi, bool *trust,
   return best;
 }
 
+// Whether a host-resident layout lies where the cost model was trained: up
+// to 4 MiB packed in a span of up to 16 MiB (tempi_b200/dispatch_train.py
+// random_layout).  Beyond that the model extrapolates, and its picks for the
+// strided sweep's host-resident points were measured 7.6 % slower than the
+// fastest candidates in total (shift kernels unpacking small rows into host
+// memory at half the speed of the word kernel).  Device layouts larger than
+// the trained 256 MiB keep the model: they are long streams, where the
+// candidates differ little, and measuring them would hold scratch memory of
+// their size.
+constexpr int64_t kTrainedHostBytes = int64_t(4) << 20;
+constexpr int64_t kTrainedHostSpan = int64_t(16) << 20;
+// Host-resident layouts are measured (on pinned scratch buffers the size of
+// their span, kept for later measurements) up to this span; beyond it the
+// fixed rules choose
+constexpr int64_t kMeasureHostSpan = int64_t(512) << 20;
+
+int64_t layout_span(const tempi_desc &d, int64_t incount) {
+  int64_t hi = d.start + d.block + (incount - 1) * d.extent;
+  for (int k = 0; k < d.ndims; ++k)
+    hi += (d.counts[k] - 1) * d.strides[k];
+  return hi;
+}
+
+enum class Range { TRAINED, MEASURE, FIXED };
+Range trained_range(const tempi_desc &d, int64_t incount, bool src_host,
+                    bool dst_host) {
+  const int64_t bytes = incount * d.size;
+  if (!src_host && !dst_host)
+    return Range::TRAINED;
+  const int64_t span = layout_span(d, incount);
+  if (bytes <= kTrainedHostBytes && span <= kTrainedHostSpan)
+    return Range::TRAINED;
+  return span <= kMeasureHostSpan ? Range::MEASURE : Range::FIXED;
+}
+
 uint64_t config_key(int64_t incount, bool src_host, bool dst_host,
                     bool unpack) {
   return (uint64_t(incount) << 3) | (unpack ? 4 : 0) | (src_host ? 2 : 0) |
@@ -431,7 +466,8 @@ tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
   bool ok[kNumConfigs];
   for (int k = 0; k < kNumConfigs; ++k)
     ok[k] = eligible(r.desc, incount, k);
-  if (mode == Dispatch::LEARNED) {
+  const Range range = trained_range(r.desc, incount, src_host, dst_host);
+  if (mode == Dispatch::LEARNED && range == Range::TRAINED) {
     float f[TEMPI_MLP_IN], mean[TEMPI_MLP_OUT], spread[TEMPI_MLP_OUT];
     features(r.desc, incount, src_host, dst_host, f);
     if (predict(f, mean, spread) == TEMPI_OK) {
@@ -450,7 +486,9 @@ tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
       }
     }
   }
-  if (mode == Dispatch::EXHAUSTIVE || (choice >= 0 && !trust)) {
+  if (mode == Dispatch::EXHAUSTIVE || (choice >= 0 && !trust) ||
+      (mode == Dispatch::LEARNED && range == Range::MEASURE)) {
+    counters().dispatch_measured++;
     float t[kMeasured];
     if (measure_candidates(r.desc, incount, src_host, dst_host, 1, 2, t) ==
         TEMPI_OK) {

@@ -51,7 +51,7 @@ struct Counters {
   std::atomic<int64_t> recv_device{0}, recv_oneshot{0}, recv_staged{0},
       recv_lib{0};
   std::atomic<int64_t> isend_managed{0}, irecv_managed{0};
-  std::atomic<int64_t> dispatch_hit{0}, dispatch_miss{0};
+  std::atomic<int64_t> dispatch_hit{0}, dispatch_miss{0}, dispatch_measured{0};
   std::atomic<int64_t> slab_hits{0}, slab_misses{0};
   // bytes held from CUDA (live + cached), handed out, kept for reuse
   std::atomic<int64_t> slab_bytes{0}, slab_live_bytes{0}, slab_cached_bytes{0};

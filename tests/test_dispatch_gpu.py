@@ -130,3 +130,36 @@ def test_layout_cache_serves_a_new_handle_of_a_known_shape(model):
     assert out.cpu().numpy().tobytes() == T.pack(o, src_np, 1).tobytes()
     mpi.Type_free(t1)
     mpi.Type_free(t2)
+
+
+def test_host_layouts_outside_training_are_measured(model):
+    """A host-resident layout beyond the model's training range (here 4 MiB
+    packed from a 64 MiB pinned span: 262,144 rows of 16 B, 256 B apart) is
+    not left to the model's extrapolation: MPI_Pack's first use times the
+    candidates (dispatch_measured moves once for the pack and the unpack
+    together), picks an eligible one, and both directions stay exact."""
+    import torch
+
+    t = mpi.Type_vector(262144, 4, 64, mpi.FLOAT)
+    assert mpi.Type_commit(t) == 0
+    err, d = mpi.describe(t)
+    assert err == 0 and d.size == 4 << 20
+    span = d.extent
+    src_np = H.splitmix_bytes(span, 17)
+    src = torch.from_numpy(src_np).pin_memory()
+    out = torch.zeros(d.size, dtype=torch.uint8).pin_memory()
+    m0 = _lib.counter("dispatch_measured")
+    e, pos = mpi.Pack(src.data_ptr(), 1, t, out.data_ptr(), out.numel())
+    assert e == 0 and pos == d.size
+    want = T.pack(T.vector(262144, 4, 64, T.FLOAT), src_np, 1)
+    assert out.numpy().tobytes() == want.tobytes()
+    assert _lib.counter("dispatch_measured") == m0 + 1
+    back = torch.full_like(src, 0xAA).pin_memory()
+    e, _ = mpi.Unpack(out.data_ptr(), out.numel(), back.data_ptr(), 1, t)
+    assert e == 0
+    exp = np.full(span, 0xAA, np.uint8)
+    T.unpack(T.vector(262144, 4, 64, T.FLOAT), want, exp, 1)
+    assert back.numpy().tobytes() == exp.tobytes()
+    # the pack's measurement chose the unpack too
+    assert _lib.counter("dispatch_measured") == m0 + 1
+    mpi.Type_free(t)
