@@ -1066,7 +1066,7 @@ def dispatch_sample(torch, n=200, seed=777):
         if DT.span_of(d, incount) > (2 << 30) or (th and DT.span_of(d, incount) > (16 << 20)):
             continue
         size = d.size * incount
-        reps = 16 if size < (1 << 20) else 6 if size < (64 << 20) else 2
+        reps = 64 if size < (1 << 20) else 16 if size < (64 << 20) else 4
         _lib.check(lib.tempi_measure(ctypes.byref(d), incount, int(th), int(ph), 1, reps, times))
         _lib.check(lib.tempi_measure(ctypes.byref(d), incount, int(th), int(ph), 1, reps, times2))
         pc, uc, mi = ctypes.c_int(-1), ctypes.c_int(-1), ctypes.c_int(0)
@@ -1134,7 +1134,7 @@ def dispatch_sample(torch, n=200, seed=777):
             "exhaustive_repeat_within_5pct": round(float(np.mean(RS <= 1.05 * RB)), 3),
             "exhaustive_repeat_total_regret": round(float(RS.sum() / RB.sum() - 1), 4),
             "exhaustive_total_us": round(float(B.sum()), 1),
-            "reps": "16 back-to-back launches per candidate under 1 MiB, 6 under 64 MiB, else 2",
+            "reps": "64 back-to-back launches per candidate under 1 MiB, 16 under 64 MiB, else 4",
             "largest_losses": worst}
 
 
