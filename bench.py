@@ -528,10 +528,11 @@ def kernel_times_from_profiles():
 def halo_bench(torch, sw, stream, reps=20):
     """The 256^3-double radius-2 halo (26 regions) and the mixed batch of 8
     grids, seeded data: plain per-region MPI_Pack / MPI_Unpack calls against
-    one batched launch and one CUDA-graph replay, the L2 flushed before each
-    timed pass.  `bit_exact`: the batched and graph outputs equal the plain
-    path's, byte for byte (compared on the device)."""
-    from tempi_b200 import halo
+    one batched launch, one CUDA-graph replay and one call of the
+    allocation-free entry point, the L2 flushed before each timed pass.
+    `bit_exact`: the batched, graph and allocation-free outputs equal the
+    plain path's, byte for byte (compared on the device)."""
+    from tempi_b200 import _lib, halo
 
     flush = lambda: sw.flush_l2(stream)
     s = stream.cuda_stream
@@ -572,10 +573,26 @@ def halo_bench(torch, sw, stream, reps=20):
         bg.replay(s)
     t_graph = time_events(torch, stream, lambda: bg.replay(s), reps, flush)
     cfg_tuned = bg.config()
+    # the allocation-free entry point: the same regions through the
+    # library's fixed device table (fill kernels + the batch kernel, no
+    # cudaMalloc and no host-to-device copy)
+    p_static = torch.zeros_like(p_plain)
+    regs = halo.regions([g], [data.data_ptr()], [p_static.data_ptr()])
+    arr = (_lib.Region * len(regs))(*regs)
+    lib = _lib.tempi()
+
+    def run_static():
+        _lib.check(lib.tempi_batch_run_static(arr, len(regs), 0, s), "tempi_batch_run_static")
+
+    for _ in range(3):
+        run_static()
+    t_static = time_events(torch, stream, run_static, reps, flush)
     torch.cuda.synchronize()
     pack_exact = bool(torch.equal(p_plain, p_batch) and torch.equal(p_plain, p_graph))
+    static_exact = bool(torch.equal(p_plain, p_static))
     b.close()
     bg.close()
+    del p_static
 
     # unpack into the ghost cells: the packed bytes land in the ghost region
     # opposite their direction, three copies of the grid, one per method
@@ -628,6 +645,7 @@ def halo_bench(torch, sw, stream, reps=20):
         "plain_us": round(1e3 * t_plain, 2), "batched_us": round(1e3 * t_batch, 2),
         "graph_us": round(1e3 * t_graph, 2),
         "graph_untuned_us": round(1e3 * t_graph_default, 2),
+        "static_us": round(1e3 * t_static, 2),
         "tuned": {"threads": cfg_tuned[0], "ctas_per_sm": cfg_tuned[1],
                   "passes_per_class": {str(k): v for k, v in cfg_tuned[2].items()}},
         "untuned": {"threads": cfg_default[0], "ctas_per_sm": cfg_default[1],
@@ -638,8 +656,9 @@ def halo_bench(torch, sw, stream, reps=20):
         "unpack_plain_us": round(1e3 * t_uplain, 2), "unpack_batched_us": round(1e3 * t_ubatch, 2),
         "unpack_graph_us": round(1e3 * t_ugraph, 2),
         "unpack_speedup_graph_vs_plain": round(t_uplain / t_ugraph, 2),
-        "bit_exact": pack_exact and unpack_exact and mixed_exact,
-        "bit_exact_parts": {"pack": pack_exact, "unpack": unpack_exact, "mixed8": mixed_exact},
+        "bit_exact": pack_exact and unpack_exact and mixed_exact and static_exact,
+        "bit_exact_parts": {"pack": pack_exact, "unpack": unpack_exact, "mixed8": mixed_exact,
+                            "static": static_exact},
         "mixed8_regions": 26 * len(grids_m), "mixed8_bytes": mixed_bytes,
         "mixed8_graph_us": round(1e3 * t_mixed, 2),
         "mixed8_plain_us": round(1e3 * t_mixed_plain, 2),
