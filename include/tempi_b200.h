@@ -199,9 +199,11 @@ int tempi_batch_create_copy(const tempi_copy_region *regions, int32_t n,
    memory from cudaMalloc.  At most 1024 regions per call (larger n returns
    TEMPI_ERR_ARG, and so does any invalid region, before anything is
    launched).  Every GPU that loads the library holds that 168 KiB array
-   until exit.  The table reaches the array through the parameters of small
-   fill kernels (one per 128 regions) launched on `stream` ahead of the
-   batch kernel, so the call copies nothing from host memory and never
+   until exit.  A table of up to 32 (non-empty) regions travels in the
+   batch kernel's own parameters (one launch, the array untouched); a
+   larger one reaches the array through the parameters of small fill
+   kernels (one per 128 regions) launched on `stream` ahead of the batch
+   kernel.  Either way the call copies nothing from host memory and never
    waits for earlier work on the stream.  The first call on a device, with
    that device current, looks up the array's device address, so make it
    before any stream capture; that address is not looked up again after a

@@ -231,14 +231,13 @@ __device__ __forceinline__ const Rec *stage_table(const Rec *__restrict__ g,
   return reinterpret_cast<const Rec *>(s_table);
 }
 
-// at least 768 threads per SM: registers are capped at 85 per thread
+// every warp chunk of the table `tab`, warps taking chunks warp_id,
+// warp_id + total warps, ...
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, (768 + THREADS - 1) / THREADS)
-    k_batch(const BatchRegion *__restrict__ regions, int nregions,
-            uint32_t total_chunks, int unpack, int staged) {
-  extern __shared__ __align__(16) uint32_t s_table[];
-  const BatchRegion *tab =
-      stage_table<BatchRegion, THREADS>(regions, nregions, staged, s_table);
+__device__ __forceinline__ void batch_chunks(const BatchRegion *tab,
+                                             int nregions,
+                                             uint32_t total_chunks,
+                                             int unpack) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nwarps = gridDim.x * (THREADS / 32);
   for (uint32_t c = blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5);
@@ -252,6 +251,17 @@ __global__ void __launch_bounds__(THREADS, (768 + THREADS - 1) / THREADS)
     default: pack_chunk_p<1>(r, c, lane, unpack); break;
     }
   }
+}
+
+// at least 768 threads per SM: registers are capped at 85 per thread
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, (768 + THREADS - 1) / THREADS)
+    k_batch(const BatchRegion *__restrict__ regions, int nregions,
+            uint32_t total_chunks, int unpack, int staged) {
+  extern __shared__ __align__(16) uint32_t s_table[];
+  const BatchRegion *tab =
+      stage_table<BatchRegion, THREADS>(regions, nregions, staged, s_table);
+  batch_chunks<THREADS>(tab, nregions, total_chunks, unpack);
 }
 
 template <int THREADS>
@@ -984,7 +994,9 @@ extern "C" int tempi_batch_config(const tempi_batch *b, int32_t *threads,
 // device should come before any stream capture.  The cached address is not
 // refreshed if the application resets the device (cudaDeviceReset).
 //
-// The table reaches the array without a host-to-device copy: the host
+// A table of up to kParamRegions entries is passed BY VALUE as the batch
+// kernel's own parameter (k_batch_param): one launch, the array untouched.
+// A larger table reaches the array without a host-to-device copy: the host
 // builds it in pieces of up to kFillPiece entries and passes each piece BY
 // VALUE as the parameter of a small kernel (k_static_fill) that writes it
 // into the array, on the caller's stream ahead of the batch kernel.  Kernel
@@ -1020,6 +1032,22 @@ __global__ void __launch_bounds__(256)
   uint32_t *to = reinterpret_cast<uint32_t *>(g_static_regions + first);
   for (int w = threadIdx.x; w < count * kWords; w += blockDim.x)
     to[w] = from[w];
+}
+
+// The allocation-free batch of up to kParamRegions regions in one launch:
+// the table travels in the kernel's parameters (5.4 KB), and each CTA copies
+// it from there into shared memory, so neither a fill kernel nor the fixed
+// array is involved.  256 threads, 3 CTAs per SM by the launch bounds.
+constexpr int kParamRegions = 32;
+
+template <int P>
+__global__ void __launch_bounds__(256, 3)
+    k_batch_param(const __grid_constant__ StaticPiece<P> piece, int nregions,
+                  uint32_t total_chunks, int unpack) {
+  extern __shared__ __align__(16) uint32_t s_table[];
+  const BatchRegion *tab =
+      stage_table<BatchRegion, 256>(piece.r, nregions, 1, s_table);
+  batch_chunks<256>(tab, nregions, total_chunks, unpack);
 }
 
 static std::mutex g_static_mu;
@@ -1080,6 +1108,24 @@ extern "C" int tempi_batch_run_static(const tempi_region *regions, int32_t n,
   int used = 0, filled = 0;
   uint64_t chunks = 0;
   for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1 && used <= kParamRegions) { // pass 0 left them all in piece
+      if (used == 0)
+        return TEMPI_OK;
+      StaticPiece<kParamRegions> small;
+      std::memcpy(small.r, piece.r, size_t(used) * sizeof(BatchRegion));
+      const uint32_t grid = std::max<uint32_t>(
+          1, std::min<uint32_t>(uint32_t((chunks + 7) / 8),
+                                uint32_t(num_sms()) * 3u));
+      k_batch_param<kParamRegions>
+          <<<grid, 256, used * int(sizeof(BatchRegion)), s>>>(
+              small, used, uint32_t(chunks), unpack ? 1 : 0);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess)
+        return cuda_error(e, "static batch launch");
+      counters().kernel_launches++;
+      set_last_kernel(unpack ? "batch_unpack_static" : "batch_pack_static");
+      return TEMPI_OK;
+    }
     used = filled = 0;
     chunks = 0;
     for (int32_t i = 0; i < n; ++i) {
