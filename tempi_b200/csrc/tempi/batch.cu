@@ -585,13 +585,68 @@ extern "C" int tempi_batch_create(const tempi_region *regions, int32_t n,
   return TEMPI_OK;
 }
 
-static int batch_launch(tempi_batch *b, cudaStream_t s) {
+template <int P> struct StaticPiece {
+  BatchRegion r[P];
+};
+
+// A batch of up to kParamRegions regions in one launch with its table in the
+// kernel's parameters (5.4 KB): each CTA copies it from there into shared
+// memory instead of from global memory.  Used by the allocation-free entry
+// point (neither a fill kernel nor the fixed array is involved) and by
+// small batches at the default launch shape.  256 threads, 3 CTAs per SM by
+// the launch bounds.
+constexpr int kParamRegions = 32;
+
+template <int P>
+__global__ void __launch_bounds__(256, 3)
+    k_batch_param(const __grid_constant__ StaticPiece<P> piece, int nregions,
+                  uint32_t total_chunks, int unpack) {
+  // read in place: a warp's region search reads one field of up to 32
+  // entries, its copy loop one entry that every lane shares
+  batch_chunks<256>(piece.r, nregions, total_chunks, unpack);
+}
+
+// k_batch_param over `n` <= kParamRegions entries of `table` (host memory),
+// `per_sm` CTAs per SM (at most 3)
+static int launch_param(const BatchRegion *table, int n, uint32_t total_chunks,
+                        int unpack, int per_sm, cudaStream_t s) {
+  StaticPiece<kParamRegions> piece;
+  std::memcpy(piece.r, table, size_t(n) * sizeof(BatchRegion));
+  const uint32_t grid = std::max<uint32_t>(
+      1, std::min<uint32_t>((total_chunks + 7) / 8,
+                            uint32_t(num_sms()) * uint32_t(per_sm)));
+  k_batch_param<kParamRegions><<<grid, 256, 0, s>>>(piece, n, total_chunks,
+                                                     unpack);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return cuda_error(e, "batch launch");
+  counters().kernel_launches++;
+  return TEMPI_OK;
+}
+
+// `direct`: a launch of its own (tempi_batch_launch).  There a small table at
+// a 256-thread shape rides in the kernel's parameters instead of being read
+// from device memory by every CTA (measured on the 256^3 halo: 11.3 against
+// 12.0-12.3 us by events, 7.3-7.6 against 7.6-7.9 us in-kernel).  Graph
+// captures and the tuner's timings keep the table in device memory: a
+// replayed kernel node with 5.4 KB of parameters measured 1-2 us slower.
+static int batch_launch(tempi_batch *b, cudaStream_t s, bool direct) {
   BatchImpl &bi = b->impl;
   if (!bi.host_pairs.empty())
     return launch_table(bi.dev_pairs, int(bi.host_pairs.size()),
                         bi.total_chunks, 0, bi.shape, s);
-  return launch_table(bi.dev, int(bi.host.size()), bi.total_chunks, bi.unpack,
-                      bi.shape, s);
+  const int n = int(bi.host.size());
+  if (direct && n > 0 && n <= kParamRegions && bi.total_chunks > 0 &&
+      (bi.shape.threads == 0 || bi.shape.threads == 256) &&
+      bi.shape.ctas_per_sm <= 3) {
+    const int per_sm = bi.shape.ctas_per_sm > 0 ? bi.shape.ctas_per_sm : 3;
+    const int err = launch_param(bi.host.data(), n, bi.total_chunks, bi.unpack,
+                                 per_sm, s);
+    if (!err)
+      set_last_kernel(bi.unpack ? "batch_unpack" : "batch_pack");
+    return err;
+  }
+  return launch_table(bi.dev, n, bi.total_chunks, bi.unpack, bi.shape, s);
 }
 
 // Copy pairs for `regions`, each at the default passes of its class; empty
@@ -732,7 +787,7 @@ int copy_batch_run(const tempi_copy_region *regions, int32_t n,
 extern "C" int tempi_batch_launch(tempi_batch *b, void *stream) {
   if (!b)
     return set_error(TEMPI_ERR_ARG, "null batch");
-  return batch_launch(b, static_cast<cudaStream_t>(stream));
+  return batch_launch(b, static_cast<cudaStream_t>(stream), true);
 }
 
 static void drop_graph(BatchImpl &bi) {
@@ -753,7 +808,7 @@ extern "C" int tempi_batch_capture(tempi_batch *b, void *stream) {
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess)
     return cuda_error(e, "begin capture");
-  int err = batch_launch(b, s);
+  int err = batch_launch(b, s, false);
   e = cudaStreamEndCapture(s, &bi.graph);
   if (err)
     return err;
@@ -789,7 +844,7 @@ float time_batch(tempi_batch *b, cudaStream_t s, const uint4 *flush,
   for (int r = 0; r < reps && !*err; ++r) {
     k_tune_flush<<<num_sms() * 8, 256, 0, s>>>(flush, flush_words, sink);
     cudaEventRecord(e0, s);
-    *err = batch_launch(b, s);
+    *err = batch_launch(b, s, false);
     cudaEventRecord(e1, s);
     if (cudaEventSynchronize(e1) != cudaSuccess) {
       *err = cuda_error(cudaGetLastError(), "tuning launch");
@@ -1013,10 +1068,6 @@ constexpr int kFillPiece = 128; // 21.5 KB of parameters (the limit is 32,764 B)
 static_assert(sizeof(BatchRegion) == 168 && sizeof(BatchRegion) % 4 == 0,
               "table entry size is documented");
 static __device__ __align__(256) BatchRegion g_static_regions[kStaticBatchRegions];
-
-template <int P> struct StaticPiece {
-  BatchRegion r[P];
-};
 static_assert(sizeof(StaticPiece<kFillPiece>) + 8 <= 32764,
               "a piece fits the kernel parameter space");
 
@@ -1032,22 +1083,6 @@ __global__ void __launch_bounds__(256)
   uint32_t *to = reinterpret_cast<uint32_t *>(g_static_regions + first);
   for (int w = threadIdx.x; w < count * kWords; w += blockDim.x)
     to[w] = from[w];
-}
-
-// The allocation-free batch of up to kParamRegions regions in one launch:
-// the table travels in the kernel's parameters (5.4 KB), and each CTA copies
-// it from there into shared memory, so neither a fill kernel nor the fixed
-// array is involved.  256 threads, 3 CTAs per SM by the launch bounds.
-constexpr int kParamRegions = 32;
-
-template <int P>
-__global__ void __launch_bounds__(256, 3)
-    k_batch_param(const __grid_constant__ StaticPiece<P> piece, int nregions,
-                  uint32_t total_chunks, int unpack) {
-  extern __shared__ __align__(16) uint32_t s_table[];
-  const BatchRegion *tab =
-      stage_table<BatchRegion, 256>(piece.r, nregions, 1, s_table);
-  batch_chunks<256>(tab, nregions, total_chunks, unpack);
 }
 
 static std::mutex g_static_mu;
@@ -1111,20 +1146,10 @@ extern "C" int tempi_batch_run_static(const tempi_region *regions, int32_t n,
     if (pass == 1 && used <= kParamRegions) { // pass 0 left them all in piece
       if (used == 0)
         return TEMPI_OK;
-      StaticPiece<kParamRegions> small;
-      std::memcpy(small.r, piece.r, size_t(used) * sizeof(BatchRegion));
-      const uint32_t grid = std::max<uint32_t>(
-          1, std::min<uint32_t>(uint32_t((chunks + 7) / 8),
-                                uint32_t(num_sms()) * 3u));
-      k_batch_param<kParamRegions>
-          <<<grid, 256, used * int(sizeof(BatchRegion)), s>>>(
-              small, used, uint32_t(chunks), unpack ? 1 : 0);
-      cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess)
-        return cuda_error(e, "static batch launch");
-      counters().kernel_launches++;
-      set_last_kernel(unpack ? "batch_unpack_static" : "batch_pack_static");
-      return TEMPI_OK;
+      err = launch_param(piece.r, used, uint32_t(chunks), unpack ? 1 : 0, 3, s);
+      if (!err)
+        set_last_kernel(unpack ? "batch_unpack_static" : "batch_pack_static");
+      return err;
     }
     used = filled = 0;
     chunks = 0;
