@@ -296,8 +296,8 @@ int pick(const float *mean, const float *spread, int lo, int hi, bool *trust,
 constexpr int64_t kTrainedHostBytes = int64_t(4) << 20;
 constexpr int64_t kTrainedHostSpan = int64_t(16) << 20;
 // Host-resident layouts are measured (on pinned scratch buffers the size of
-// their span, kept for later measurements) up to this span; beyond it the
-// fixed rules choose
+// their span, freed again afterwards) up to this span; beyond it the fixed
+// rules choose
 constexpr int64_t kMeasureHostSpan = int64_t(512) << 20;
 
 int64_t layout_span(const tempi_desc &d, int64_t incount) {
@@ -490,8 +490,11 @@ tempi_config choose_config(TypeRecord &r, int64_t incount, bool src_host,
       (mode == Dispatch::LEARNED && range == Range::MEASURE)) {
     counters().dispatch_measured++;
     float t[kMeasured];
-    if (measure_candidates(r.desc, incount, src_host, dst_host, 1, 2, t) ==
-        TEMPI_OK) {
+    const int me = measure_candidates(r.desc, incount, src_host, dst_host, 1, 2, t);
+    // a choice made at run time holds no scratch memory afterwards (its
+    // buffers are the size of the layout's span)
+    measure_release();
+    if (me == TEMPI_OK) {
       int best = -1;
       for (int j = 0; j < kNumConfigs; ++j)
         if (std::isfinite(t[lo + j]) && (best < 0 || t[lo + j] < t[lo + best]))

@@ -74,6 +74,9 @@ void dispatch_init();
 // `what`: bit 0 configurations, bit 1 methods.
 int measure_candidates(const tempi_desc &d, int64_t incount, bool src_host,
                        bool dst_host, int what, int reps, float *times_us);
+// Free the scratch buffers measure_candidates keeps between calls (the
+// training harness reuses them; a one-off measurement need not hold them).
+void measure_release();
 
 // Forced method for measurement (-1: none)
 void force_method(int m);

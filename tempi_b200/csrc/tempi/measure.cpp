@@ -94,6 +94,15 @@ int build_type(const tempi_desc &d, MPI_Datatype *out) {
 
 } // namespace
 
+void measure_release() {
+  std::lock_guard<std::mutex> l(g_mu);
+  for (Buf *b : {&g_typed[0], &g_typed[1], &g_typed2, &g_packed[0], &g_packed[1]}) {
+    if (b->p)
+      b->host ? cudaFreeHost(b->p) : cudaFree(b->p);
+    *b = Buf{};
+  }
+}
+
 int measure_candidates(const tempi_desc &d, int64_t incount, bool src_host,
                        bool dst_host, int what, int reps, float *times) {
   for (int j = 0; j < kMeasured; ++j)
