@@ -356,6 +356,9 @@ def main(argv=None):
     ap.add_argument("--out", default=None)
     ap.add_argument("--reps", default=None,
                     help="launches per candidate under 1 MiB,64 MiB,above (default 12,6,2)")
+    ap.add_argument("--dataset", default=None,
+                    help="train on a dispatch_dataset.npz saved by an earlier run instead of "
+                         "measuring (same --seed and --types)")
     ap.add_argument("--no-install", action="store_true",
                     help="do not write tempi_b200/models/")
     args = ap.parse_args(argv)
@@ -368,7 +371,11 @@ def main(argv=None):
     assert mpi.Init() == 0
     gpu = torch.cuda.get_device_name(0)
     print(f"measuring up to {args.types} layouts on {gpu} (budget {args.budget_s:.0f} s)")
-    X, T, meta, t_meas = measure_dataset(args.types, args.budget_s, args.seed)
+    if args.dataset:
+        z = np.load(args.dataset)
+        X, T, meta, t_meas = z["X"], z["T"], z["meta"], 0.0
+    else:
+        X, T, meta, t_meas = measure_dataset(args.types, args.budget_s, args.seed)
     n = len(X)
     h = min(args.heldout, n // 10)
     # regenerate the held-out descriptors for the table policy
